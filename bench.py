@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 epsilon-grid self-join (algorithm 3 drop-in).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Workload (default): the 2-D low-dimensional large workload - 20M points, 90%
+from 64 isotropic Gaussians + 10% uniform background in [0,1000)^2, eps set
+for about 32 neighbours per point, STAMP=1 (synthetic, seeded; see
+gpu_self_join_b200/synth.py).  A step is one complete self-join of the
+workload: index build, count pass, offsets, fill pass (the full neighbour
+table).
+
+Metric: result pairs per second (R / step time), whole job over N GPUs.
+  value  - inputs resident in HBM, results left in HBM (device-timed: CUDA
+           events on the current stream around K back-to-back steps; the
+           input, 160 MB, and the working set exceed the 126 MB L2).
+  e2e    - the same metric through the public API with host buffers: H2D of
+           the pinned input, the join, D2H of numNeighbors and neighborTable
+           into pinned host memory, every step.
+Multi-GPU: "replicas only" - every rank joins its own copy (no data-path
+collective); value = pairs of all ranks / max-over-ranks time.
+
+--impl reference times the reference's own CPU implementation of the path on
+this host's cores, on a bounded query sample of the same workload (see
+_reference_arm).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def _env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ helpers
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_from_profile(kernel: str, workload: str):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for ln in f:
+            if ln.startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(ln.split(":", 1)[1].strip().split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def _cpu_baseline(pts: np.ndarray, w, budget_s: float = 15.0) -> dict:
+    """The oracle's grid join (a CPU port of algorithm 3) on a bounded query
+    sample of the same workload, all host threads: index over all N points,
+    then the sampled queries; pairs/s is extrapolated to the full join."""
+    from oracle import pyoracle as O
+
+    O.lib()
+    N = pts.shape[0]
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(12345)
+    cfg = O.OracleConfig(k=w.k, reorder=w.reorder, ilp=w.ilp, shortcircuit=w.shortcircuit, nthreads=cores)
+    nq = 20000
+    q = np.sort(rng.choice(N, size=nq, replace=False)).astype(np.uint32)
+    tot, si, sq = O.join_sample(pts, w.eps, cfg, q)
+    # grow the sample to fill the budget
+    per_q = sq / nq
+    nq2 = int(min(N, max(nq, (budget_s - si) / max(per_q, 1e-9))))
+    if nq2 > nq * 2:
+        q = np.sort(rng.choice(N, size=nq2, replace=False)).astype(np.uint32)
+        tot, si, sq = O.join_sample(pts, w.eps, cfg, q)
+        nq = nq2
+    est_R = tot * (N / nq)
+    est_t = si + sq * (N / nq)
+    return {"value": est_R / est_t, "unit": "pairs/s", "cores": cores, "kind": "port",
+            "sample": f"grid index over all {N} points ({si:.2f} s) + {nq} seeded queries ({sq:.2f} s); "
+                      f"pairs/s extrapolated to all {N} queries"}
+
+
+# ------------------------------------------------------------------ our arm
+def _ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from gpu_self_join_b200 import JoinConfig, SelfJoin, synth
+
+    rank, local_rank, world = _env_rank()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    w = synth.WORKLOADS[args.workload]
+    pts = synth.generate(args.workload)
+    N, n = pts.shape
+    cfg = JoinConfig(indexed_dims=w.k, reorder=w.reorder, shortcircuit=w.shortcircuit, ilp=w.ilp, stamp=w.stamp,
+                     query_reorder=w.query_reorder)
+    sj = SelfJoin(local_rank)
+    x_dev = torch.from_numpy(pts).cuda()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- value: device-resident input and result
+    for _ in range(args.warmup):
+        sj.run(x_dev, w.eps, cfg)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    stats = []
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        stats.append(sj.run(x_dev, w.eps, cfg))
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    R = stats[-1]["total_pairs"]
+    pairs_local = R * args.steps
+    ms_max, pairs_all = ms, pairs_local
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        p = torch.tensor([pairs_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        pairs_all = float(p.item())
+    value = pairs_all / (ms_max / 1e3)
+
+    # ---- roofline of the dominant kernel
+    fill_ms = statistics.mean(s["dev_ms_fill"] for s in stats)
+    count_ms = statistics.mean(s["dev_ms_count"] for s in stats)
+    peak, peak_kind = _peaks()
+    b_coords = 4.0 * N * n
+    bytes_fill = b_coords + 4.0 * N + 8.0 * N + 4.0 * R
+    bytes_count = b_coords + 4.0 * N + 4.0 * N + (4.0 * N if w.stamp else 0.0)
+    if fill_ms >= count_ms:
+        kname, kms, kbytes = "join_fill", fill_ms, bytes_fill
+    else:
+        kname, kms, kbytes = "join_count", count_ms, bytes_count
+    achieved = kbytes / (kms / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes": kbytes,
+            "kernel_ms": kms, "traffic": _traffic_from_profile(kname, args.workload),
+            "stage_ms": {"index": statistics.mean(s["dev_ms_index"] for s in stats), "count": count_ms,
+                         "fill": fill_ms}}
+
+    # ---- e2e: host buffers through the public API
+    e2e = None
+    if not args.no_e2e:
+        h_in = torch.from_numpy(pts).pin_memory().numpy()
+        h_counts = torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+        h_table = torch.empty(max(R, 1), dtype=torch.int32).pin_memory().numpy().view(np.uint32)[:R]
+        for _ in range(max(1, min(args.warmup, 2))):
+            sj.run(h_in, w.eps, cfg)
+            sj.counts(out=h_counts)
+            sj.table(out=h_table)
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(args.steps):
+            sj.run(h_in, w.eps, cfg)
+            sj.counts(out=h_counts)
+            sj.table(out=h_table)
+        f1.record()
+        torch.cuda.synchronize()
+        barrier()
+        ems = f0.elapsed_time(f1)
+        if world > 1:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": pairs_all / (ems / 1e3), "unit": "pairs/s", "ms_per_step": ems / args.steps,
+               "h2d_bytes_per_step": int(N * n * 4), "d2h_bytes_per_step": int(4 * N + 4 * R)}
+
+    launches = int(sum(s.get("kernel_launches", 0) for s in stats))
+    line = {
+        "metric": "self-join result pairs/s (2-D, 20M points, STAMP=1)" if args.workload == "c2_gmm2d"
+        else f"self-join result pairs/s ({args.workload})",
+        "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded, shapes/distributions of the benchmark workload)",
+        "config": {"workload": args.workload, "points": N, "dim": n, "eps": w.eps, "indexed_dims": w.k,
+                   "stamp": w.stamp, "reorder": w.reorder, "ilp": w.ilp, "shortcircuit": w.shortcircuit,
+                   "query_reorder": w.query_reorder, "result_pairs_per_step": R,
+                   "candidates_per_step": stats[-1]["candidates"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs (160 MB) and working set larger than L2"},
+        "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = _cpu_baseline(pts, w)
+        except Exception as ex:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(ex)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sj.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ reference arm
+def _reference_arm(args) -> None:
+    """The reference's CPU implementation of the self-join on a bounded sample
+    of the same workload, with all host threads.  Uses the reference's R-tree
+    search + filter (tree_index.cpp:191-233, RTree.h) built from its sources
+    into oracle/_ref/rtree_harness when present, else the oracle port."""
+    rank, _, world = _env_rank()
+    if rank != 0:
+        return
+    from gpu_self_join_b200 import synth
+
+    w = synth.WORKLOADS[args.workload]
+    pts = synth.generate(args.workload)
+    N, n = pts.shape
+    harness = os.path.join(ROOT, "oracle", "_ref", "rtree_harness")
+    vals = []
+    desc = None
+    kind = "port"
+    cores = os.cpu_count() or 1
+    for step in range(args.warmup + args.steps):
+        if os.path.exists(harness):
+            kind = "reference"
+            r = _run_rtree_harness(harness, pts, w, cores, seed=step)
+            v, desc = r["value"], r["sample"]
+        else:
+            r = _cpu_baseline(pts, w, budget_s=10.0)
+            v, desc = r["value"], r["sample"]
+        if step >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {"impl": "reference", "metric": "self-join result pairs/s (2-D, 20M points, STAMP=1)"
+            if args.workload == "c2_gmm2d" else f"self-join result pairs/s ({args.workload})",
+            "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": {"workload": args.workload, "points": N, "dim": n, "eps": w.eps},
+            "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _run_rtree_harness(harness, pts, w, cores, seed):
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as td:
+        f = os.path.join(td, "pts.bin")
+        pts.tofile(f)
+        out = subprocess.run([harness, f, str(pts.shape[0]), str(pts.shape[1]), repr(float(w.eps)), str(cores),
+                              "8.0", str(seed)], capture_output=True, text=True, check=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2_gmm2d")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        _reference_arm(args)
+    else:
+        _ours(args)
+
+
+if __name__ == "__main__":
+    main()

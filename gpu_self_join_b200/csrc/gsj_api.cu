@@ -1,0 +1,823 @@
+// Host orchestration and C ABI of the B200 self-join (include/gpuselfjoin.h).
+//
+// One gsj_join() call replaces the mode-3 body of main.cu:178-262 together
+// with distanceTableNDGridBatches (GPU.cu:270-1088) and the table export of
+// main.cu:514-542:
+//   H2D of the dataset (when it lives on the host)
+//   REORDER statistic on the device, dimension order on the host (std::sort
+//     with the reference comparator, main.cu:1040)
+//   grid extents: device min/max, scalar tail on the host (main.cu:925-946)
+//   index: cell keys -> radix sort -> runs -> cell table -> work items
+//   count pass -> list offsets (scan) -> fill pass  (the neighbour table)
+// The result stays on the device in the context's pool until fetched.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_run_length_encode.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "../../include/gpuselfjoin.h"
+#include "gsj_common.cuh"
+#include "gsj_kernels.h"
+#include "gsj_scan.h"
+
+// Build-time defaults, same macro names as the reference's params.h.
+#ifndef GPUNUMDIM
+#define GPUNUMDIM 0 /* 0: any dimensionality accepted at run time */
+#endif
+#ifndef NUMINDEXEDDIM
+#define NUMINDEXEDDIM 6
+#endif
+#ifndef REORDER
+#define REORDER 0
+#endif
+#ifndef SHORTCIRCUIT
+#define SHORTCIRCUIT 0
+#endif
+#ifndef ILP
+#define ILP 0
+#endif
+#ifndef STAMP
+#define STAMP 0
+#endif
+#ifndef QUERYREORDER
+#define QUERYREORDER 0
+#endif
+
+using namespace gsj;
+
+namespace {
+
+struct Buf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+// Model of the distance arithmetic from the ILP / SHORTCIRCUIT switches.
+int model_of(const gsj_config& c) {
+    if (c.ilp == 0) return kSeq;
+    return c.shortcircuit ? kIlpSc : kIlp;
+}
+
+template <typename T>
+T threshold_of(T eps);
+
+template <>
+float threshold_of<float>(float eps) {
+    if (std::isnan(eps) || eps < 0.0f) return -INFINITY;
+    if (std::isinf(eps)) return INFINITY;
+    float s = (float)((double)eps * (double)eps);
+    while (s > 0.0f && std::sqrt(s) > eps) s = std::nextafter(s, 0.0f);
+    for (;;) {
+        const float nx = std::nextafter(s, INFINITY);
+        if (std::sqrt(nx) <= eps) s = nx;
+        else break;
+    }
+    return s;
+}
+
+template <>
+double threshold_of<double>(double eps) {
+    if (std::isnan(eps) || eps < 0.0) return -INFINITY;
+    if (std::isinf(eps)) return INFINITY;
+    double s = eps * eps;
+    if (std::isinf(s)) s = DBL_MAX;
+    while (s > 0.0 && std::sqrt(s) > eps) s = std::nextafter(s, 0.0);
+    for (;;) {
+        const double nx = std::nextafter(s, INFINITY);
+        if (std::sqrt(nx) <= eps) s = nx;
+        else break;
+    }
+    return s;
+}
+
+template <typename T>
+struct dim_reorder_sort {  // structs.h:37-41
+    unsigned int dim;
+    T variance;
+};
+template <typename T>
+bool compareByDimVariance(const dim_reorder_sort<T>& a, const dim_reorder_sort<T>& b) {  // main.cu:33-36
+    return a.variance > b.variance;
+}
+
+uint32_t npad_of(uint32_t n, uint32_t tsize) {
+    return n <= 2 ? n : ((n + (16u / tsize) - 1u) / (16u / tsize)) * (16u / tsize);
+}
+
+}  // namespace
+
+struct gsj_context {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaEvent_t tev[6] = {};  // stage timing: index start/end, count start/end, fill start/end
+    // device pool
+    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, hkeys, hvals, order, sizes, nchunks,
+        item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
+        minmax_part;
+    PinnedBuf stage[2];
+    PinnedBuf hmisc;
+    // last result
+    bool have_result = false;
+    uint64_t N = 0, R = 0;
+    std::string err;
+    gsj_stats stats{};
+};
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err_default;
+
+int fail(gsj_context* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err_default = msg;
+    return code;
+}
+
+#define GSJ_CUDA(ctx, call)                                                                               \
+    do {                                                                                                  \
+        cudaError_t _e = (call);                                                                          \
+        if (_e != cudaSuccess)                                                                            \
+            return fail((ctx), _e == cudaErrorMemoryAllocation ? GSJ_ERR_NOMEM : GSJ_ERR_CUDA,            \
+                        std::string(#call) + ": " + cudaGetErrorString(_e));                              \
+    } while (0)
+
+// Grow-only device allocation.
+template <typename X>
+int dev_get(gsj_context* c, Buf& b, size_t count, X** out) {
+    const size_t bytes = std::max<size_t>(count * sizeof(X), 256);
+    if (b.cap < bytes) {
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        size_t want = bytes + bytes / 8;  // headroom for slightly larger repeats
+        cudaError_t e = cudaMalloc(&b.p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            e = cudaMalloc(&b.p, bytes);
+            want = bytes;
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GSJ_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+        }
+        b.cap = want;
+    }
+    *out = static_cast<X*>(b.p);
+    return GSJ_OK;
+}
+
+int pinned_get(gsj_context* c, PinnedBuf& b, size_t bytes) {
+    if (b.cap < bytes) {
+        if (b.p) cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+        if (cudaMallocHost(&b.p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, GSJ_ERR_NOMEM, "pinned host allocation failed");
+        }
+        b.cap = bytes;
+    }
+    return GSJ_OK;
+}
+
+#define GSJ_TRY(x)                    \
+    do {                              \
+        int _r = (x);                 \
+        if (_r != GSJ_OK) return _r;  \
+    } while (0)
+
+bool host_is_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// Parallel host memcpy (the copy-out of staged results into pageable memory).
+void par_memcpy(void* dst, const void* src, size_t bytes) {
+    const size_t kMin = 8u << 20;
+    unsigned nt = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 16u);
+    if (bytes < kMin || nt == 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t per = (bytes + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+        const size_t b = t * per;
+        if (b >= bytes) break;
+        const size_t len = std::min(per, bytes - b);
+        th.emplace_back([=] { std::memcpy((char*)dst + b, (const char*)src + b, len); });
+    }
+    for (auto& x : th) x.join();
+}
+
+// Device -> host copy through two pinned staging buffers on alternating
+// streams, so the PCIe transfer of chunk i+1 overlaps the copy-out of chunk i.
+int d2h_staged(gsj_context* c, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return GSJ_OK;
+    if (host_is_pinned(dst)) {
+        GSJ_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->st));
+        GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+        return GSJ_OK;
+    }
+    const size_t chunk = 64u << 20;
+    GSJ_TRY(pinned_get(c, c->stage[0], chunk));
+    GSJ_TRY(pinned_get(c, c->stage[1], chunk));
+    const size_t nch = (bytes + chunk - 1) / chunk;
+    cudaStream_t ss[2] = {c->st, c->st2};
+    for (size_t i = 0; i < nch && i < 2; i++) {
+        const size_t off = i * chunk, len = std::min(chunk, bytes - off);
+        GSJ_CUDA(c, cudaMemcpyAsync(c->stage[i].p, (const char*)src + off, len, cudaMemcpyDeviceToHost, ss[i]));
+        GSJ_CUDA(c, cudaEventRecord(c->ev[i], ss[i]));
+    }
+    for (size_t i = 0; i < nch; i++) {
+        const int b = (int)(i & 1);
+        const size_t off = i * chunk, len = std::min(chunk, bytes - off);
+        GSJ_CUDA(c, cudaEventSynchronize(c->ev[b]));
+        par_memcpy((char*)dst + off, c->stage[b].p, len);
+        const size_t nx = i + 2;
+        if (nx < nch) {
+            const size_t off2 = nx * chunk, len2 = std::min(chunk, bytes - off2);
+            GSJ_CUDA(c, cudaMemcpyAsync(c->stage[b].p, (const char*)src + off2, len2, cudaMemcpyDeviceToHost, ss[b]));
+            GSJ_CUDA(c, cudaEventRecord(c->ev[b], ss[b]));
+        }
+    }
+    return GSJ_OK;
+}
+
+int h2d_copy(gsj_context* c, void* dst, const void* src, size_t bytes) {
+    GSJ_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->st));
+    return GSJ_OK;
+}
+
+template <typename X>
+int d2h_small(gsj_context* c, X* dst, const X* src, size_t count) {
+    GSJ_CUDA(c, cudaMemcpyAsync(dst, src, count * sizeof(X), cudaMemcpyDeviceToHost, c->st));
+    GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+    return GSJ_OK;
+}
+
+int validate(gsj_context* c, const gsj_config& cfg, uint64_t N) {
+    if (cfg.dim == 0) return fail(c, GSJ_ERR_INVALID, "dim must be >= 1");
+    if (cfg.dim > 4096) return fail(c, GSJ_ERR_INVALID, "dim above 4096 is not supported");
+    if (cfg.indexed_dims == 0 || cfg.indexed_dims > cfg.dim)
+        return fail(c, GSJ_ERR_INVALID, "indexed_dims must satisfy 1 <= k <= dim (main.cu:70)");
+    if (cfg.indexed_dims > 8) return fail(c, GSJ_ERR_INVALID, "indexed_dims above 8 is not supported");
+    if (cfg.ilp > (uint32_t)kMaxIlp) return fail(c, GSJ_ERR_INVALID, "ILP above 64 is not supported");
+    if (cfg.dtype != GSJ_FLOAT32 && cfg.dtype != GSJ_FLOAT64) return fail(c, GSJ_ERR_INVALID, "unknown dtype");
+    if (N >= (1ull << 31)) return fail(c, GSJ_ERR_INVALID, "at most 2^31-1 points per join");
+    return GSJ_OK;
+}
+
+// ------------------------------------------------------------------ join
+template <typename T>
+int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const gsj_config& cfg, int on_dev) {
+    const double t_start = now_ms();
+    gsj_stats& S = c->stats;
+    S = gsj_stats{};
+    S.num_points = N;
+    c->have_result = false;
+    c->N = N;
+    c->R = 0;
+    const T eps = (T)eps_d;
+    const uint32_t n = cfg.dim, k = cfg.indexed_dims;
+    const uint32_t npad = npad_of(n, sizeof(T));
+    cudaStream_t st = c->st;
+
+    uint32_t *counts = nullptr;
+    uint64_t* offsets = nullptr;
+    GSJ_TRY(dev_get(c, c->counts, N + 1, &counts));
+    GSJ_TRY(dev_get(c, c->offsets, N + 1, &offsets));
+    if (N == 0) {
+        GSJ_CUDA(c, cudaMemsetAsync(offsets, 0, sizeof(uint64_t), st));
+        GSJ_CUDA(c, cudaStreamSynchronize(st));
+        c->have_result = true;
+        S.ms_total = now_ms() - t_start;
+        return GSJ_OK;
+    }
+
+    // ---- input
+    const T* d_in = nullptr;
+    if (on_dev) {
+        d_in = static_cast<const T*>(data);
+    } else {
+        T* p = nullptr;
+        GSJ_TRY(dev_get(c, c->in, N * n, &p));
+        const double t0 = now_ms();
+        GSJ_TRY(h2d_copy(c, p, data, N * n * sizeof(T)));
+        GSJ_CUDA(c, cudaStreamSynchronize(st));
+        S.ms_h2d = now_ms() - t0;
+        d_in = p;
+    }
+    const double t_index = now_ms();
+    GSJ_CUDA(c, cudaEventRecord(c->tev[0], st));
+
+    // ---- REORDER (main.cu:981-1075): statistic on the device, order on the host
+    std::vector<uint32_t> perm(n);
+    for (uint32_t j = 0; j < n; j++) perm[j] = j;
+    if (cfg.reorder) {
+        T* d_var = nullptr;
+        GSJ_TRY(dev_get(c, c->var, n, &d_var));
+        const T inv_sample = (T)(1.0 / (100 * 1.0));
+        const T denom = (T)N * inv_sample;
+        S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_variance<T>(d_in, N, n, denom, d_var, st));
+        std::vector<T> var(n);
+        GSJ_TRY(d2h_small(c, var.data(), d_var, n));
+        std::vector<dim_reorder_sort<T>> dv(n);
+        for (uint32_t j = 0; j < n; j++) dv[j] = {j, var[j]};
+        std::sort(dv.begin(), dv.end(), compareByDimVariance<T>);
+        for (uint32_t j = 0; j < n; j++) perm[j] = dv[j].dim;
+    }
+    uint32_t* d_perm = nullptr;
+    GSJ_TRY(dev_get(c, c->perm, n, &d_perm));
+    GSJ_CUDA(c, cudaMemcpyAsync(d_perm, perm.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+
+    // ---- grid extents (main.cu:891-948)
+    const uint32_t nparts = (uint32_t)std::min<uint64_t>((N + 255) / 256, (uint64_t)c->num_sms * 4);
+    T *d_part = nullptr, *d_mm = nullptr;
+    GSJ_TRY(dev_get(c, c->minmax_part, (size_t)nparts * 2 * k, &d_part));
+    GSJ_TRY(dev_get(c, c->misc, 2 * kMaxK + 8, &d_mm));
+    S.kernel_launches += 2;
+    GSJ_CUDA(c, launch_minmax<T>(d_in, N, n, k, d_perm, d_part, nparts, d_mm, st));
+    std::vector<T> mm(2 * k);
+    GSJ_TRY(d2h_small(c, mm.data(), d_mm, 2 * k));
+    std::vector<T> minArr(k), maxArr(k);
+    GridGeom g{};
+    g.k = k;
+    uint64_t totalCells = 1;
+    if (!(eps > T(0)) || std::isinf(eps))
+        return fail(c, GSJ_ERR_INVALID, "epsilon must be positive and finite");
+    long double cells_prod = 1.0L;
+    for (uint32_t j = 0; j < k; j++) {
+        minArr[j] = mm[j] - eps;
+        maxArr[j] = mm[k + j] + eps;
+        const T q = (maxArr[j] - minArr[j]) / eps;
+        const T cq = std::ceil(q);
+        if (!(cq >= T(1)) || !(cq < T(4294967296.0)))
+            return fail(c, GSJ_ERR_INVALID, "grid dimension out of range (non-finite data or epsilon too small)");
+        g.ncells[j] = (uint32_t)cq;
+        cells_prod *= (long double)g.ncells[j];
+    }
+    // the reference's uint64 linear ids (main.cu:867-883) alias once the grid
+    // has 2^64 cells or more; such grids are rejected instead
+    if (cells_prod >= 18446744073709551615.0L)
+        return fail(c, GSJ_ERR_INVALID, "grid has 2^64 cells or more (epsilon too small for this data)");
+    uint64_t mult = 1;
+    for (uint32_t j = 0; j < k; j++) {
+        g.mult[j] = mult;
+        mult *= g.ncells[j];
+        totalCells = (j == 0) ? g.ncells[0] : totalCells * g.ncells[j];
+    }
+    S.total_cells = totalCells;
+    T* d_min = nullptr;
+    GSJ_TRY(dev_get(c, c->minarr, k, &d_min));
+    GSJ_CUDA(c, cudaMemcpyAsync(d_min, minArr.data(), k * sizeof(T), cudaMemcpyHostToDevice, st));
+
+    // ---- cell keys + radix sort (subsystem (a))
+    uint64_t *keys = nullptr, *keys2 = nullptr;
+    uint32_t *vals = nullptr, *ids = nullptr;
+    GSJ_TRY(dev_get(c, c->keys, N, &keys));
+    GSJ_TRY(dev_get(c, c->keys2, N, &keys2));
+    GSJ_TRY(dev_get(c, c->vals, N, &vals));
+    GSJ_TRY(dev_get(c, c->ids, N, &ids));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_cell_keys<T>(d_in, N, n, d_perm, g, d_min, eps, keys, vals, st));
+    int bits = 1;
+    while (bits < 64 && (totalCells - 1) >> bits) bits++;
+    size_t tb = 0;
+    GSJ_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, vals, ids, (int)N, 0, bits, st));
+    void* temp = nullptr;
+    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+    GSJ_CUDA(c, cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, ids, (int)N, 0, bits, st));
+
+    // ---- runs of equal keys = non-empty cells
+    uint64_t* cell_key = nullptr;
+    uint32_t *runs = nullptr, *cell_start = nullptr, *d_nruns = nullptr;
+    GSJ_TRY(dev_get(c, c->cell_key, N, &cell_key));
+    GSJ_TRY(dev_get(c, c->runs, N + 1, &runs));
+    GSJ_TRY(dev_get(c, c->cell_start, N + 1, &cell_start));
+    d_nruns = reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK);
+    GSJ_CUDA(c, cub::DeviceRunLengthEncode::Encode(nullptr, tb, keys2, cell_key, runs, d_nruns, (int)N, st));
+    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+    GSJ_CUDA(c, cub::DeviceRunLengthEncode::Encode(temp, tb, keys2, cell_key, runs, d_nruns, (int)N, st));
+    uint32_t M = 0;
+    GSJ_TRY(d2h_small(c, &M, d_nruns, 1));
+    S.nonempty_cells = M;
+    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tb, runs, cell_start, (int)M, st));
+    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(temp, tb, runs, cell_start, (int)M, st));
+
+    // ---- points in cell order
+    T* pts = nullptr;
+    GSJ_TRY(dev_get(c, c->pts, N * npad, &pts));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_gather_points<T>(d_in, N, n, npad, d_perm, ids, pts, st));
+
+    // ---- cell lookup: dense table when the grid is small, else a hash table
+    uint32_t* dense = nullptr;
+    unsigned long long* hkeys = nullptr;
+    uint32_t* hvals = nullptr;
+    uint64_t hmask = 0;
+    const uint64_t dense_limit = std::max<uint64_t>(1u << 24, 4ull * N);
+    if (totalCells <= dense_limit && totalCells <= (1ull << 30)) {
+        GSJ_TRY(dev_get(c, c->dense, totalCells, &dense));
+        GSJ_CUDA(c, cudaMemsetAsync(dense, 0, totalCells * sizeof(uint32_t), st));
+    } else {
+        uint64_t hcap = 1024;
+        while (hcap < 2ull * M) hcap <<= 1;
+        hmask = hcap - 1;
+        GSJ_TRY(dev_get(c, c->hkeys, hcap, &hkeys));
+        GSJ_TRY(dev_get(c, c->hvals, hcap, &hvals));
+        GSJ_CUDA(c, cudaMemsetAsync(hkeys, 0xff, hcap * sizeof(unsigned long long), st));
+    }
+    S.kernel_launches += 2;
+    GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, M, (uint32_t)N, dense, hkeys, hvals, hmask, st));
+
+    // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525)
+    uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
+    GSJ_TRY(dev_get(c, c->nchunks, M + 1, &nchunks));
+    GSJ_TRY(dev_get(c, c->item_off, M + 1, &item_off));
+    if (cfg.query_reorder) {
+        uint32_t *sizes = nullptr, *sizes2 = nullptr, *iota = nullptr;
+        GSJ_TRY(dev_get(c, c->sizes, 2 * (size_t)M, &sizes));
+        sizes2 = sizes + M;
+        GSJ_TRY(dev_get(c, c->order, 2 * (size_t)M, &order));
+        iota = order + M;
+        S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, nchunks, sizes, st));
+        S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_iota(iota, M, st));
+        // stable descending sort by cell size: ties keep ascending cell order
+        GSJ_CUDA(c, cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, sizes, sizes2, iota, order, (int)M, 0, 32,
+                                                              st));
+        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+        GSJ_CUDA(c, cub::DeviceRadixSort::SortPairsDescending(temp, tb, sizes, sizes2, iota, order, (int)M, 0, 32,
+                                                              st));
+        S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_item_counts(cell_start, order, M, nchunks, nullptr, st));
+    } else {
+        S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, nchunks, nullptr, st));
+    }
+    GSJ_CUDA(c, cudaMemsetAsync(nchunks + M, 0, sizeof(uint32_t), st));
+    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tb, nchunks, item_off, (int)M + 1, st));
+    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(temp, tb, nchunks, item_off, (int)M + 1, st));
+    uint32_t num_items = 0;
+    GSJ_TRY(d2h_small(c, &num_items, item_off + M, 1));
+    S.work_items = num_items;
+    uint2* items = nullptr;
+    GSJ_TRY(dev_get(c, c->items, num_items, &items));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_make_items(order, nchunks, item_off, M, items, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[1], st));
+    GSJ_CUDA(c, cudaStreamSynchronize(st));
+    const double t_join = now_ms();
+    S.ms_index = t_join - t_index;
+
+    // ---- count pass
+    uint32_t *fwd = nullptr, *rev = nullptr;
+    GSJ_TRY(dev_get(c, c->fwd, N, &fwd));
+    GSJ_TRY(dev_get(c, c->rev, N, &rev));
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK) + 2;  // work counter
+    unsigned long long* cand = reinterpret_cast<unsigned long long*>(reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK) + 4);
+    GSJ_CUDA(c, cudaMemsetAsync(rev, 0, N * sizeof(uint32_t), st));
+    GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, 4 * sizeof(uint32_t), st));
+    JoinArgs<T> a{};
+    a.pts = pts;
+    a.ids = ids;
+    a.cell_start = cell_start;
+    a.cell_key = cell_key;
+    a.dense = dense;
+    a.hkeys = reinterpret_cast<const uint64_t*>(hkeys);
+    a.hvals = hvals;
+    a.hmask = hmask;
+    a.items = items;
+    a.num_items = num_items;
+    a.work_counter = ctr;
+    a.n = n;
+    a.npad = npad;
+    a.ilp = cfg.ilp;
+    a.g = g;
+    a.thr = threshold_of<T>(eps);
+    a.fwd_cnt = fwd;
+    a.rev_cnt = rev;
+    a.cand_cnt = cand;
+    const int model = model_of(cfg);
+    const bool stamp = cfg.stamp != 0;
+    GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_join<T>(a, kCount, model, stamp, c->num_sms, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
+
+    // ---- list lengths and offsets
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_sum_counts(fwd, rev, N, counts, st));
+    void* stemp = nullptr;
+    GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
+    S.kernel_launches += 3;
+    GSJ_CUDA(c, scan_u32_u64(counts, offsets, N, stemp, st));
+    uint64_t R = 0;
+    GSJ_TRY(d2h_small(c, &R, offsets + N, 1));
+    unsigned long long ncand = 0;
+    GSJ_TRY(d2h_small(c, &ncand, cand, 1));
+    S.candidates = ncand;
+
+    // ---- fill pass
+    unsigned long long* revcur = nullptr;
+    uint32_t* table = nullptr;
+    GSJ_TRY(dev_get(c, c->revcur, N, &revcur));
+    GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_rev_cursor(offsets, fwd, N, revcur, st));
+    GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st));
+    a.offsets = offsets;
+    a.rev_cursor = revcur;
+    a.table = table;
+    a.table_cap = R;
+    a.err_flag = ctr + 1;  // zeroed with the counters before the count pass
+    GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_join<T>(a, kFill, model, stamp, c->num_sms, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
+    GSJ_CUDA(c, cudaStreamSynchronize(st));
+    {
+        float ms = 0;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
+        S.dev_ms_index = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[2], c->tev[3]));
+        S.dev_ms_count = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[4], c->tev[5]));
+        S.dev_ms_fill = ms;
+    }
+    uint32_t errflag = 0;
+    GSJ_TRY(d2h_small(c, &errflag, ctr + 1, 1));
+    if (errflag) return fail(c, GSJ_ERR_STATE, "fill pass disagreed with the count pass (table bound reached)");
+    S.ms_join = now_ms() - t_join;
+    S.total_pairs = R;
+    c->R = R;
+    c->have_result = true;
+    S.ms_total = now_ms() - t_start;
+    return GSJ_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+static std::mutex g_cfg_mu;
+static bool g_cfg_set = false;
+static gsj_config g_cfg;
+
+void gsj_default_config(gsj_config* cfg) {
+    if (!cfg) return;
+    {
+        std::lock_guard<std::mutex> lk(g_cfg_mu);
+        if (g_cfg_set) {
+            *cfg = g_cfg;
+            return;
+        }
+    }
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->dim = GPUNUMDIM;
+    cfg->indexed_dims = NUMINDEXEDDIM;
+#ifdef GSJ_DTYPE_DOUBLE
+    cfg->dtype = GSJ_FLOAT64;
+#else
+    cfg->dtype = GSJ_FLOAT32;
+#endif
+    cfg->reorder = REORDER;
+    cfg->shortcircuit = SHORTCIRCUIT;
+    cfg->ilp = ILP;
+    cfg->stamp = STAMP;
+    cfg->query_reorder = QUERYREORDER;
+    cfg->device = 0;
+    cfg->flags = GSJ_FLAG_QUIET;
+}
+
+int gsj_set_default_config(const gsj_config* cfg) {
+    if (!cfg) return fail(nullptr, GSJ_ERR_INVALID, "null config");
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    g_cfg = *cfg;
+    g_cfg_set = true;
+    return GSJ_OK;
+}
+
+int gsj_create(gsj_context** out, int device) {
+    if (!out) return fail(nullptr, GSJ_ERR_INVALID, "null context pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, GSJ_ERR_CUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(nullptr, GSJ_ERR_INVALID, "device ordinal out of range");
+    gsj_context* c = new gsj_context();
+    c->device = device;
+    GSJ_CUDA(c, cudaSetDevice(device));
+    GSJ_CUDA(c, cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    GSJ_CUDA(c, cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    GSJ_CUDA(c, cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+    GSJ_CUDA(c, cudaEventCreateWithFlags(&c->ev[0], cudaEventDisableTiming));
+    GSJ_CUDA(c, cudaEventCreateWithFlags(&c->ev[1], cudaEventDisableTiming));
+    for (auto& e : c->tev) GSJ_CUDA(c, cudaEventCreate(&e));
+    *out = c;
+    return GSJ_OK;
+}
+
+int gsj_destroy(gsj_context* c) {
+    if (!c) return GSJ_OK;
+    cudaSetDevice(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->st2) cudaStreamSynchronize(c->st2);
+    Buf* bufs[] = {&c->in,       &c->pts,   &c->ids,    &c->keys,      &c->keys2,   &c->vals,      &c->cell_key,
+                   &c->runs,     &c->cell_start, &c->dense, &c->hkeys, &c->hvals,   &c->order,     &c->sizes,
+                   &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
+                   &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
+                   &c->minarr,   &c->minmax_part};
+    for (Buf* b : bufs)
+        if (b->p) cudaFree(b->p);
+    for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})
+        if (pb->p) cudaFreeHost(pb->p);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->tev)
+        if (e) cudaEventDestroy(e);
+    if (c->st) cudaStreamDestroy(c->st);
+    if (c->st2) cudaStreamDestroy(c->st2);
+    delete c;
+    return GSJ_OK;
+}
+
+int gsj_join(gsj_context* c, const void* data, uint64_t num_points, double eps, const gsj_config* cfg,
+             int data_on_device, gsj_stats* stats) {
+    if (!c || !cfg) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (!data && num_points) return fail(c, GSJ_ERR_INVALID, "null data");
+    GSJ_TRY(validate(c, *cfg, num_points));
+    if (cfg->device != c->device) return fail(c, GSJ_ERR_INVALID, "config device differs from the context's device");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    int r = cfg->dtype == GSJ_FLOAT32 ? run_join<float>(c, data, num_points, eps, *cfg, data_on_device)
+                                      : run_join<double>(c, data, num_points, eps, *cfg, data_on_device);
+    if (stats) *stats = c->stats;
+    return r;
+}
+
+int gsj_result_size(gsj_context* c, uint64_t* total) {
+    if (!c || !total) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (!c->have_result) return fail(c, GSJ_ERR_STATE, "no join result");
+    *total = c->R;
+    return GSJ_OK;
+}
+
+int gsj_result_counts(gsj_context* c, uint32_t* out, int dst_on_device) {
+    if (!c || (!out && c->N)) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (!c->have_result) return fail(c, GSJ_ERR_STATE, "no join result");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    if (c->N == 0) return GSJ_OK;
+    if (dst_on_device) {
+        GSJ_CUDA(c, cudaMemcpyAsync(out, c->counts.p, c->N * 4, cudaMemcpyDeviceToDevice, c->st));
+        GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+        return GSJ_OK;
+    }
+    const double t0 = now_ms();
+    int r = d2h_staged(c, out, c->counts.p, c->N * 4);
+    c->stats.ms_d2h += now_ms() - t0;
+    return r;
+}
+
+int gsj_result_table(gsj_context* c, uint32_t* out, uint64_t cap, int dst_on_device) {
+    if (!c || (!out && c->R)) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (!c->have_result) return fail(c, GSJ_ERR_STATE, "no join result");
+    if (cap < c->R) return fail(c, GSJ_ERR_INVALID, "destination smaller than the result");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    if (c->R == 0) return GSJ_OK;
+    if (dst_on_device) {
+        GSJ_CUDA(c, cudaMemcpyAsync(out, c->table.p, c->R * 4, cudaMemcpyDeviceToDevice, c->st));
+        GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+        return GSJ_OK;
+    }
+    const double t0 = now_ms();
+    int r = d2h_staged(c, out, c->table.p, c->R * 4);
+    c->stats.ms_d2h += now_ms() - t0;
+    return r;
+}
+
+int gsj_result_device(gsj_context* c, const uint32_t** counts, const uint64_t** offsets, const uint32_t** table) {
+    if (!c) return fail(c, GSJ_ERR_INVALID, "null context");
+    if (!c->have_result) return fail(c, GSJ_ERR_STATE, "no join result");
+    if (counts) *counts = static_cast<const uint32_t*>(c->counts.p);
+    if (offsets) *offsets = static_cast<const uint64_t*>(c->offsets.p);
+    if (table) *table = static_cast<const uint32_t*>(c->table.p);
+    return GSJ_OK;
+}
+
+const char* gsj_last_error(gsj_context* c) {
+    if (c) return c->err.c_str();
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_err_default.c_str();
+}
+
+float gsj_threshold_f32(float eps) { return threshold_of<float>(eps); }
+double gsj_threshold_f64(double eps) { return threshold_of<double>(eps); }
+
+// ---------------------------------------------------------------- drop-in
+static std::mutex g_py_mu;
+static gsj_context* g_py_ctx = nullptr;
+static bool g_py_pending = false;
+
+static int py_join(const void* dataset, unsigned int N, double eps, unsigned int NDIM, int dev, uint32_t dtype,
+                   unsigned int* outNum) {
+    std::lock_guard<std::mutex> lk(g_py_mu);
+    gsj_config cfg;
+    gsj_default_config(&cfg);
+    if (cfg.dim != 0 && NDIM != cfg.dim) {
+        std::fprintf(stderr, "\nERROR: GPUNUMDIM=%u of this library differs from NDIM=%u\n", cfg.dim, NDIM);
+        return fail(nullptr, GSJ_ERR_INVALID, "NDIM differs from the library's GPUNUMDIM");
+    }
+    cfg.dim = NDIM;
+    cfg.dtype = dtype;
+    cfg.device = dev;
+    if (cfg.indexed_dims > NDIM) cfg.indexed_dims = NDIM;
+    if (g_py_ctx && g_py_ctx->device != dev) {
+        gsj_destroy(g_py_ctx);
+        g_py_ctx = nullptr;
+    }
+    if (!g_py_ctx) GSJ_TRY(gsj_create(&g_py_ctx, dev));
+    g_py_pending = false;
+    GSJ_TRY(gsj_join(g_py_ctx, dataset, N, eps, &cfg, 0, nullptr));
+    GSJ_TRY(gsj_result_counts(g_py_ctx, outNum, 0));
+    g_py_pending = true;
+    return GSJ_OK;
+}
+
+int GDSJoinPy_f32(const float* dataset, unsigned int N, float eps, unsigned int NDIM, int dev, unsigned int* out) {
+    return py_join(dataset, N, eps, NDIM, dev, GSJ_FLOAT32, out);
+}
+int GDSJoinPy_f64(const double* dataset, unsigned int N, double eps, unsigned int NDIM, int dev, unsigned int* out) {
+    return py_join(dataset, N, eps, NDIM, dev, GSJ_FLOAT64, out);
+}
+
+void GDSJoinPy(gsj_dtype_t* dataset, unsigned int NUMPOINTS, gsj_dtype_t epsilon, unsigned int NDIM, int gpuContext,
+               unsigned int* outNumNeighborsWithinEps) {
+#ifdef GSJ_DTYPE_DOUBLE
+    int r = GDSJoinPy_f64(dataset, NUMPOINTS, epsilon, NDIM, gpuContext, outNumNeighborsWithinEps);
+#else
+    int r = GDSJoinPy_f32(dataset, NUMPOINTS, epsilon, NDIM, gpuContext, outNumNeighborsWithinEps);
+#endif
+    if (r != GSJ_OK) std::fprintf(stderr, "\nGDSJoinPy: %s\n", gsj_last_error(nullptr));
+}
+
+int copyResultIntoPythonArray64(unsigned int* out, uint64_t numResults) {
+    std::lock_guard<std::mutex> lk(g_py_mu);
+    if (!g_py_ctx || !g_py_pending) return fail(nullptr, GSJ_ERR_STATE, "no pending GDSJoinPy result");
+    if (numResults > g_py_ctx->R) return fail(nullptr, GSJ_ERR_INVALID, "numResults exceeds the result size");
+    int r = GSJ_OK;
+    if (numResults) {
+        GSJ_CUDA(g_py_ctx, cudaSetDevice(g_py_ctx->device));
+        r = d2h_staged(g_py_ctx, out, g_py_ctx->table.p, numResults * 4);
+    }
+    g_py_pending = false;
+    return r;
+}
+
+void copyResultIntoPythonArray(unsigned int* out, unsigned int numResults) {
+    int r = copyResultIntoPythonArray64(out, numResults);
+    if (r != GSJ_OK) std::fprintf(stderr, "\ncopyResultIntoPythonArray: %s\n", gsj_last_error(nullptr));
+}
+
+}  // extern "C"

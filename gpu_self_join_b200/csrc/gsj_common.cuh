@@ -1,0 +1,69 @@
+// Shared definitions of the B200 epsilon-grid self-join kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gsj {
+
+constexpr int kMaxK = 10;        // indexed dimensions supported (3^10 neighbour offsets)
+constexpr int kMaxIlp = 64;      // ILP register blocks supported
+constexpr int kQChunk = 32;      // queries per work item (one per lane)
+constexpr uint32_t kCrossBit = 0x80000000u;  // neighbour entry visited across cells (unicomp)
+constexpr uint64_t kEmptyKey = ~0ull;        // hash table empty slot
+
+// Arithmetic order of the squared-distance sum, i.e. the reference's
+// ILP/SHORTCIRCUIT switches (kernel.cu:307-377):
+//   kSeq    ILP==0                  s = fma(d, d, s) over l = 0..n-1
+//   kIlp    ILP>0,  SHORTCIRCUIT=0  r_j = fma(d, d, r_j) for l = j (mod ILP); s = r_0 + r_1 + ...
+//   kIlpSc  ILP>0,  SHORTCIRCUIT=1  per ILP block: s = fma(d_l, d_l, s); s += d_{l+j}^2 (j >= 1)
+enum Model : int { kSeq = 0, kIlp = 1, kIlpSc = 2 };
+
+enum Pass : int { kCount = 0, kFill = 1 };
+
+// Grid geometry (k <= kMaxK indexed dims).
+struct GridGeom {
+    uint32_t k;
+    uint32_t ncells[kMaxK];
+    uint64_t mult[kMaxK];  // linear id stride of dim j (dim 0 fastest, main.cu:867-883)
+};
+
+template <typename T>
+struct JoinArgs {
+    const T* pts;                 // [N][npad] points in cell order, columns reordered
+    const uint32_t* ids;          // [N] slot -> original point id
+    const uint32_t* cell_start;   // [M+1]
+    const uint64_t* cell_key;     // [M]
+    const uint32_t* dense;        // [totalCells] cell index + 1 (0 = empty), or null
+    const uint64_t* hkeys;        // [hcap] hash table keys (kEmptyKey = empty), or null
+    const uint32_t* hvals;        // [hcap] cell indices
+    uint64_t hmask;               // hcap - 1
+    const uint2* items;           // [num_items] (cell, chunk)
+    uint32_t num_items;
+    uint32_t* work_counter;       // dynamic work distribution
+    uint32_t n, npad, ilp;
+    GridGeom g;
+    T thr;                        // s <= thr  <=>  sqrt(s) <= eps
+    // count pass
+    uint32_t* fwd_cnt;            // [N] by original id
+    uint32_t* rev_cnt;            // [N] by original id (unicomp reverse hits)
+    unsigned long long* cand_cnt; // candidate evaluations
+    // fill pass
+    const uint64_t* offsets;      // [N+1] by original id
+    unsigned long long* rev_cursor;  // [N] next free reverse slot by original id
+    uint32_t* table;              // [R]
+    unsigned long long table_cap; // R: writes at or beyond it are dropped and flagged
+    uint32_t* err_flag;           // set to 1 when a write would leave the table
+};
+
+__host__ __device__ inline uint64_t mix64(uint64_t x) {
+    // splitmix64 finaliser: hash of a linear cell id
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+}  // namespace gsj

@@ -1,0 +1,373 @@
+// Candidate-cell distance join (subsystem (b)).
+//
+// Replaces kernelNDGridIndexGlobal / evaluateCell / evalPoint
+// (kernel.cu:132-480, kernelloops.h, stamploops.h).  The reference runs one
+// thread per query point, repeats the neighbour-cell search (2 binary searches
+// per cell) for every query, and appends every hit with a global atomicAdd.
+// Here one warp owns a work item: up to 32 consecutive query slots of one
+// non-empty cell.  The warp
+//   1. enumerates the cell's 3^k neighbour offsets once, lanes in parallel,
+//      resolving each through the dense cell table or the hash table, and
+//      compacts the non-empty ones (ballot) into a per-warp list in shared
+//      memory - with STAMP only the unicomp half-space of stamploops.h;
+//   2. stages the queries in shared memory;
+//   3. walks the concatenated candidate slots 32 at a time, one candidate per
+//      lane (rows are contiguous in the cell-sorted layout), and tests every
+//      query against the 32 candidates with the reference's exact arithmetic
+//      (s <= thr is sqrt(s) <= eps, see gsj_threshold_*).
+// Pass kCount counts hits per query (and, with STAMP, reverse hits per
+// candidate).  Pass kFill recomputes and writes each hit straight into its
+// final neighbour-table position: forward hits of query j land contiguously
+// at a warp-uniform cursor (ballot + popc, one coalesced store per hit),
+// reverse hits of a candidate are placed through one atomic reservation per
+// (candidate, work item).  No pair buffer and no key sort are needed
+// (kernel.cu:367-375 + GPU.cu:863-980 in the reference).
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gsj_common.cuh"
+#include "gsj_fp.cuh"
+#include "gsj_kernels.h"
+
+namespace gsj {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__host__ __device__ constexpr uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
+
+__host__ __device__ constexpr uint32_t npad_for(uint32_t n, uint32_t tsize) {
+    return n <= 2 ? n : ((n + (16u / tsize) - 1u) / (16u / tsize)) * (16u / tsize);
+}
+
+struct WarpSmem {
+    uint32_t q_off, qid_off, nbs_off, nbp_off, cand_off, total;
+};
+
+__host__ __device__ inline WarpSmem warp_smem_layout(uint32_t npad, uint32_t tsize, uint32_t nb_cap, bool generic) {
+    WarpSmem w{};
+    uint32_t o = 0;
+    w.q_off = o;
+    o = align16(o + 32u * npad * tsize);
+    w.qid_off = o;
+    o = align16(o + 32u * 4u);
+    w.nbs_off = o;
+    o = align16(o + nb_cap * 4u);
+    w.nbp_off = o;
+    o = align16(o + (nb_cap + 1u) * 4u);
+    w.cand_off = o;
+    if (generic) o = align16(o + 32u * (npad + 1u) * tsize);
+    w.total = o;
+    return w;
+}
+
+template <typename T>
+__device__ __forceinline__ int lookup_cell(const JoinArgs<T>& a, uint64_t lin) {
+    if (a.dense) return (int)a.dense[lin] - 1;
+    uint64_t h = mix64(lin) & a.hmask;
+    for (uint64_t p = 0; p <= a.hmask; p++) {
+        const uint64_t kk = a.hkeys[h];
+        if (kk == lin) return (int)a.hvals[h];
+        if (kk == kEmptyKey) return -1;
+        h = (h + 1) & a.hmask;
+    }
+    return -1;
+}
+
+// Squared distance in the reference's order with the candidate row in
+// registers (NT = n known at compile time; sequential model only).
+template <typename T, int NT>
+__device__ __forceinline__ T sqdist_seq_reg(const T* __restrict__ q, const T (&c)[NT]) {
+    T s = T(0);
+#pragma unroll
+    for (int l = 0; l < NT; l++) {
+        const T d = FP<T>::sub(c[l], q[l]);
+        s = FP<T>::fma(d, d, s);
+    }
+    return s;
+}
+
+// Generic n: candidate row and query row in shared memory.  `alive` is the
+// lane's vote input for the warp-wide early exit; an exit never changes a
+// decision because every model's running sum only grows once it is above thr.
+template <typename T, int MODEL>
+__device__ __forceinline__ T sqdist_generic(const T* __restrict__ q, const T* __restrict__ c, uint32_t n,
+                                            uint32_t ilp, T thr, bool valid) {
+    const unsigned FULL = 0xffffffffu;
+    if (MODEL == kSeq) {
+        T s = T(0);
+        for (uint32_t l = 0; l < n; l++) {
+            const T d = FP<T>::sub(c[l], q[l]);
+            s = FP<T>::fma(d, d, s);
+            if ((l & 7u) == 7u && __all_sync(FULL, !valid || s > thr)) break;
+        }
+        return s;
+    } else if (MODEL == kIlp) {
+        // runningDist[j] accumulates dims l == j (mod ILP); then summed in j order (kernel.cu:312-341)
+        T s = T(0);
+        for (uint32_t j = 0; j < ilp; j++) {
+            T r = T(0);
+            for (uint32_t l = j; l < n; l += ilp) {
+                const T d = FP<T>::sub(c[l], q[l]);
+                r = FP<T>::fma(d, d, r);
+            }
+            s = (j == 0) ? r : FP<T>::add(s, r);
+        }
+        return s;
+    } else {
+        // SHORTCIRCUIT with ILP: per block, the first dim is fused into the
+        // running total, the others are squared separately and added in order.
+        T s = T(0);
+        for (uint32_t l = 0; l < n; l += ilp) {
+            T d = FP<T>::sub(c[l], q[l]);
+            s = FP<T>::fma(d, d, s);
+            for (uint32_t j = 1; j < ilp && l + j < n; j++) {
+                d = FP<T>::sub(c[l + j], q[l + j]);
+                s = FP<T>::add(s, FP<T>::mul(d, d));
+            }
+            if (__all_sync(FULL, !valid || s > thr)) break;
+        }
+        return s;
+    }
+}
+
+template <typename T, int NT, int MODEL, bool STAMP, int PASS>
+__global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool GENERIC = (NT == 0);
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const uint32_t npad = a.npad;
+    const WarpSmem L = warp_smem_layout(npad, sizeof(T), nb_cap, GENERIC);
+    unsigned char* wb = smem_raw + (size_t)warp * L.total;
+    T* q_s = reinterpret_cast<T*>(wb + L.q_off);
+    uint32_t* qid_s = reinterpret_cast<uint32_t*>(wb + L.qid_off);
+    uint32_t* nb_start = reinterpret_cast<uint32_t*>(wb + L.nbs_off);
+    uint32_t* nb_pref = reinterpret_cast<uint32_t*>(wb + L.nbp_off);
+    T* cand_s = reinterpret_cast<T*>(wb + L.cand_off);
+    const unsigned lt = lanemask_lt();
+    const uint32_t k = a.g.k;
+    unsigned long long cand_total = 0;
+
+    for (;;) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= a.num_items) break;
+        const uint2 wi = a.items[item];
+        const uint32_t cell = wi.x;
+        const uint32_t cs = a.cell_start[cell], ce = a.cell_start[cell + 1];
+        const uint32_t q0 = cs + wi.y * kQChunk;
+        const uint32_t qn = min((uint32_t)kQChunk, ce - q0);
+
+        // ---- own cell coordinates from the linear id
+        uint32_t own[kMaxK];
+        const uint64_t key = a.cell_key[cell];
+#pragma unroll
+        for (int j = 0; j < kMaxK; j++) own[j] = (j < (int)k) ? (uint32_t)((key / a.g.mult[j]) % a.g.ncells[j]) : 0u;
+
+        // ---- neighbour cells (kernel.cu:180-303; stamploops.h for STAMP)
+        uint32_t nnb = 0;
+        for (uint32_t base = 0; base < noff; base += 32) {
+            const uint32_t o = base + lane;
+            bool ok = o < noff;
+            uint64_t lin = 0;
+            bool moved = false, hd_odd = false;
+            uint32_t t = o;
+#pragma unroll
+            for (int j = 0; j < kMaxK; j++) {
+                if (j < (int)k) {
+                    const int dl = (int)(t % 3u) - 1;
+                    t /= 3u;
+                    const long long nbj = (long long)own[j] + dl;
+                    if (nbj < 0 || nbj >= (long long)a.g.ncells[j]) ok = false;
+                    lin += (uint64_t)nbj * a.g.mult[j];
+                    if (dl != 0) {
+                        moved = true;
+                        hd_odd = (own[j] & 1u) != 0;  // highest differing dim wins
+                    }
+                }
+            }
+            // unicomp: a neighbour whose highest differing dim d has an even own
+            // coordinate is visited from the other cell (stamploops.h: `nDCellIDs[d] & 1`)
+            if (STAMP && moved && !hd_odd) ok = false;
+            const bool cross = STAMP && moved;
+            int c = -1;
+            if (ok) c = lookup_cell(a, lin);
+            const bool found = c >= 0;
+            const unsigned m = __ballot_sync(FULL, found);
+            if (found) {
+                const uint32_t pos = nnb + __popc(m & lt);
+                const uint32_t st = a.cell_start[c];
+                nb_start[pos] = st | (cross ? kCrossBit : 0u);
+                nb_pref[pos] = a.cell_start[c + 1] - st;
+            }
+            nnb += __popc(m);
+        }
+        __syncwarp();
+        // exclusive prefix of candidate counts over the list
+        uint32_t run = 0;
+        for (uint32_t base = 0; base < nnb; base += 32) {
+            const uint32_t i = base + lane;
+            const uint32_t v = i < nnb ? nb_pref[i] : 0u;
+            uint32_t x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, x, o);
+                if (lane >= o) x += y;
+            }
+            if (i < nnb) nb_pref[i] = run + x - v;
+            run += __shfl_sync(FULL, x, 31);
+        }
+        const uint32_t total = run;
+        if (lane == 0) nb_pref[nnb] = total;
+
+        // ---- queries
+        for (uint32_t e = lane; e < qn * npad; e += 32) q_s[e] = a.pts[(size_t)q0 * npad + e];
+        if (lane < qn) qid_s[lane] = a.ids[q0 + lane];
+        __syncwarp();
+        if (PASS == kCount) cand_total += (unsigned long long)total * qn;
+        uint32_t myq = 0;
+        unsigned long long mycur = 0;
+        if (PASS == kFill && lane < qn) mycur = a.offsets[qid_s[lane]];
+
+        // ---- candidate tiles
+        uint32_t ent = 0;
+        for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+            const uint32_t f = t0 + lane;
+            const bool valid = f < total;
+            uint32_t slot = 0, corig = 0;
+            bool cross = false;
+            if (valid) {
+                while (nb_pref[ent + 1] <= f) ent++;
+                const uint32_t st = nb_start[ent];
+                cross = (st & kCrossBit) != 0u;
+                slot = (st & ~kCrossBit) + (f - nb_pref[ent]);
+                corig = a.ids[slot];
+            }
+            T creg[NT > 0 ? NT : 1];
+            if (!GENERIC) {
+                const T* row = a.pts + (size_t)slot * npad;
+#pragma unroll
+                for (int l = 0; l < (NT > 0 ? NT : 1); l++) creg[l] = row[l];
+            } else {
+                const T* row = a.pts + (size_t)slot * npad;
+                T* dst = cand_s + (size_t)lane * (npad + 1u);
+                for (uint32_t l = 0; l < a.n; l++) dst[l] = row[l];
+                __syncwarp();
+            }
+            uint32_t myrev = 0, revmask = 0;
+            for (uint32_t j = 0; j < qn; j++) {
+                const T* q = q_s + (size_t)j * npad;
+                T s;
+                if (!GENERIC) {
+                    if constexpr (NT > 0) s = sqdist_seq_reg<T, NT>(q, creg);
+                } else {
+                    s = sqdist_generic<T, MODEL>(q, cand_s + (size_t)lane * (npad + 1u), a.n, a.ilp, a.thr, valid);
+                }
+                const bool hit = valid && (s <= a.thr);
+                const unsigned b = __ballot_sync(FULL, hit);
+                if (PASS == kCount) {
+                    if (lane == (int)j) myq += __popc(b);
+                    if (STAMP && cross && hit) myrev++;
+                } else {
+                    const unsigned long long cur = __shfl_sync(FULL, mycur, j);
+                    if (hit) {
+                        const unsigned long long pos = cur + __popc(b & lt);
+                        if (pos < a.table_cap) a.table[pos] = corig;
+                        else *a.err_flag = 1u;
+                    }
+                    if (lane == (int)j) mycur += __popc(b);
+                    if (STAMP && cross && hit) revmask |= 1u << j;
+                }
+            }
+            if (PASS == kCount) {
+                if (STAMP && myrev) atomicAdd(&a.rev_cnt[corig], myrev);
+            } else if (STAMP && revmask) {
+                unsigned long long pos = atomicAdd(&a.rev_cursor[corig], (unsigned long long)__popc(revmask));
+                while (revmask) {
+                    const int j = __ffs(revmask) - 1;
+                    revmask &= revmask - 1u;
+                    if (pos < a.table_cap) a.table[pos] = qid_s[j];
+                    else *a.err_flag = 1u;
+                    pos++;
+                }
+            }
+            __syncwarp();
+        }
+        if (PASS == kCount && lane < qn) a.fwd_cnt[qid_s[lane]] = myq;
+        __syncwarp();
+    }
+    if (PASS == kCount && lane == 0 && cand_total) atomicAdd(a.cand_cnt, cand_total);
+}
+
+// ------------------------------------------------------------------ launch
+template <typename T, int NT, int MODEL, bool STAMP, int PASS>
+static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, int num_sms, cudaStream_t st) {
+    auto kern = k_join<T, NT, MODEL, STAMP, PASS>;
+    const WarpSmem L = warp_smem_layout(a.npad, sizeof(T), nb_cap, NT == 0);
+    const uint32_t max_smem = 200u * 1024u;
+    int warps = (int)(max_smem / L.total);
+    if (warps > 8) warps = 8;
+    if (warps < 1) return cudaErrorInvalidValue;
+    const int threads = warps * 32;
+    const size_t smem = (size_t)warps * L.total;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const uint64_t needed = ((uint64_t)a.num_items + warps - 1) / warps;
+    uint64_t blocks = (uint64_t)num_sms * per_sm;
+    if (blocks > needed) blocks = needed ? needed : 1;
+    kern<<<(unsigned)blocks, threads, smem, st>>>(a, nb_cap, noff);
+    return cudaGetLastError();
+}
+
+template <typename T, int MODEL, bool STAMP, int PASS>
+static cudaError_t dispatch_nt(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, int num_sms, cudaStream_t st) {
+    if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
+        switch (a.n) {
+            case 2: return launch_one<T, 2, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 3: return launch_one<T, 3, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 4: return launch_one<T, 4, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 6: return launch_one<T, 6, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 8: return launch_one<T, 8, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            default: break;
+        }
+    }
+    return launch_one<T, 0, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+}
+
+template <typename T, bool STAMP, int PASS>
+static cudaError_t dispatch_model(const JoinArgs<T>& a, int model, uint32_t nb_cap, uint32_t noff, int num_sms,
+                                  cudaStream_t st) {
+    switch (model) {
+        case kSeq: return dispatch_nt<T, kSeq, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kIlp: return dispatch_nt<T, kIlp, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kIlpSc: return dispatch_nt<T, kIlpSc, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T>
+cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, int num_sms, cudaStream_t st) {
+    uint32_t noff = 1;
+    for (uint32_t j = 0; j < a.g.k; j++) noff *= 3u;
+    const uint32_t nb_cap = noff;
+    if (pass == kCount)
+        return stamp ? dispatch_model<T, true, kCount>(a, model, nb_cap, noff, num_sms, st)
+                     : dispatch_model<T, false, kCount>(a, model, nb_cap, noff, num_sms, st);
+    return stamp ? dispatch_model<T, true, kFill>(a, model, nb_cap, noff, num_sms, st)
+                 : dispatch_model<T, false, kFill>(a, model, nb_cap, noff, num_sms, st);
+}
+
+template cudaError_t launch_join<float>(const JoinArgs<float>&, int, int, bool, int, cudaStream_t);
+template cudaError_t launch_join<double>(const JoinArgs<double>&, int, int, bool, int, cudaStream_t);
+
+}  // namespace gsj

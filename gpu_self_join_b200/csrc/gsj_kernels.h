@@ -1,0 +1,42 @@
+// Host-side launchers of the self-join kernels (internal interface between
+// gsj_api.cu and the kernel translation units).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gsj_common.cuh"
+
+namespace gsj {
+
+constexpr unsigned kVarStageBytes = 32768;  // shared staging of sampled rows (REORDER statistic)
+
+template <typename T>
+cudaError_t launch_variance(const T* in, uint64_t N, uint32_t n, T denom, T* var_out, cudaStream_t st);
+template <typename T>
+cudaError_t launch_minmax(const T* in, uint64_t N, uint32_t n, uint32_t k, const uint32_t* perm, T* part,
+                          uint32_t nparts, T* out, cudaStream_t st);
+template <typename T>
+cudaError_t launch_cell_keys(const T* in, uint64_t N, uint32_t n, const uint32_t* perm, const GridGeom& g,
+                             const T* minArr, T eps, uint64_t* keys, uint32_t* vals, cudaStream_t st);
+template <typename T>
+cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t npad, const uint32_t* perm,
+                                 const uint32_t* ids, T* pts, cudaStream_t st);
+cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, uint32_t M, uint32_t N,
+                               uint32_t* dense, unsigned long long* hkeys, uint32_t* hvals, uint64_t hmask,
+                               cudaStream_t st);
+cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t* nchunks,
+                               uint32_t* sizes, cudaStream_t st);
+cudaError_t launch_make_items(const uint32_t* order, const uint32_t* nchunks, const uint32_t* item_off,
+                              uint32_t M, uint2* items, cudaStream_t st);
+cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st);
+cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, uint64_t N, uint32_t* total,
+                              cudaStream_t st);
+cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, uint64_t N, unsigned long long* cur,
+                              cudaStream_t st);
+
+// Join passes.  `pass` is kCount or kFill; `model` one of Model; `stamp`
+// selects the unicomp traversal.  The launcher picks the specialisation.
+template <typename T>
+cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, int num_sms, cudaStream_t st);
+
+}  // namespace gsj

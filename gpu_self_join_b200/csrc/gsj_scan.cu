@@ -1,0 +1,117 @@
+// Exclusive prefix sum of 32-bit counts into 64-bit offsets (subsystem (d)):
+// the per-point list offsets of the neighbour table.  Replaces the
+// reference's key sort + kernelUniqueKeys + second sort + host range
+// stitching (GPU.cu:863-980, kernel.cu:79-105, GPU.cu:1143-1214): with exact
+// per-point counts the table is laid out by one scan.
+//
+// Three phases over tiles of kScanTile elements: tile sums, a single-block
+// scan of the tile sums, and the tile-local scans with the tile prefix added.
+// out has n+1 entries; out[n] is the total.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gsj_scan.h"
+
+namespace gsj {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr uint64_t kScanTile = (uint64_t)kScanThreads * kScanItems;
+
+__device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the exclusive
+// prefix and writes the block total to *total.
+__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long* total) {
+    __shared__ unsigned long long wsum[kScanThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned long long inc = warp_incl_scan(v, lane);
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long w = lane < kScanThreads / 32 ? wsum[lane] : 0ull;
+        w = warp_incl_scan(w, lane);
+        if (lane < kScanThreads / 32) wsum[lane] = w;
+    }
+    __syncthreads();
+    const unsigned long long before = warp ? wsum[warp - 1] : 0ull;
+    *total = wsum[kScanThreads / 32 - 1];
+    __syncthreads();
+    return before + inc - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_sums(const uint32_t* __restrict__ in, uint64_t n,
+                                                            unsigned long long* __restrict__ tsum) {
+    const uint64_t base = blockIdx.x * kScanTile;
+    unsigned long long s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const uint64_t e = base + (uint64_t)i * kScanThreads + threadIdx.x;
+        if (e < n) s += in[e];
+    }
+    unsigned long long tot;
+    block_excl_scan(s, &tot);
+    if (threadIdx.x == 0) tsum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(unsigned long long* __restrict__ tsum,
+                                                                 uint64_t ntiles) {
+    unsigned long long carry = 0;
+    for (uint64_t b0 = 0; b0 < ntiles; b0 += kScanThreads) {
+        const uint64_t i = b0 + threadIdx.x;
+        const unsigned long long v = i < ntiles ? tsum[i] : 0ull;
+        unsigned long long tot;
+        const unsigned long long ex = block_excl_scan(v, &tot);
+        if (i < ntiles) tsum[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) tsum[ntiles] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint32_t* __restrict__ in, uint64_t n,
+                                                            const unsigned long long* __restrict__ tsum,
+                                                            uint64_t ntiles, uint64_t* __restrict__ out) {
+    // each thread owns kScanItems consecutive elements of the tile
+    const uint64_t base = blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    unsigned long long s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const uint64_t e = base + i;
+        v[i] = e < n ? in[e] : 0u;
+        s += v[i];
+    }
+    unsigned long long tot;
+    unsigned long long run = block_excl_scan(s, &tot) + tsum[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const uint64_t e = base + i;
+        if (e < n) out[e] = run;
+        run += v[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tsum[ntiles];
+}
+
+size_t scan_u32_u64_temp_bytes(uint64_t n) { return ((n + kScanTile - 1) / kScanTile + 1) * sizeof(unsigned long long); }
+
+cudaError_t scan_u32_u64(const uint32_t* in, uint64_t* out, uint64_t n, void* temp, cudaStream_t st) {
+    const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    unsigned long long* tsum = static_cast<unsigned long long*>(temp);
+    if (ntiles == 0) {
+        cudaError_t e = cudaMemsetAsync(out, 0, sizeof(uint64_t), st);
+        return e;
+    }
+    k_tile_sums<<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, tsum);
+    k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(tsum, ntiles);
+    k_tile_scan<<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, tsum, ntiles, out);
+    return cudaGetLastError();
+}
+
+}  // namespace gsj

@@ -1,0 +1,148 @@
+"""Context-based Python API over the C ABI (include/gpuselfjoin.h).
+
+    with SelfJoin(device=0) as sj:
+        stats = sj.run(points, eps, indexed_dims=2, stamp=True)
+        counts, table = sj.counts(), sj.table()
+
+``points`` is an N x n float32/float64 numpy array (host) or a CUDA torch
+tensor (device-resident input, no host copy).  Results stay on the device
+until fetched; ``counts_offsets_table_device`` returns them as CUDA torch
+tensors without a host round trip.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+
+
+@dataclass
+class JoinConfig:
+    """The reference's params.h switches that shape a join (params.h:17-93)."""
+
+    indexed_dims: int = 6     # NUMINDEXEDDIM (clamped to n)
+    reorder: bool = False     # REORDER
+    shortcircuit: bool = False  # SHORTCIRCUIT
+    ilp: int = 0              # ILP
+    stamp: bool = False       # STAMP
+    query_reorder: bool = False  # QUERYREORDER
+    sort_lists: bool = False  # sort each neighbour list ascending
+
+
+class SelfJoin:
+    def __init__(self, device: int = 0):
+        self._L = N.lib()
+        self._ctx = ctypes.c_void_p()
+        N.check(self._L.gsj_create(ctypes.byref(self._ctx), int(device)))
+        self.device = int(device)
+        self.n = 0
+        self.N = 0
+
+    def close(self) -> None:
+        if self._ctx:
+            self._L.gsj_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _cfg(self, n: int, dtype, cfg: JoinConfig) -> N.GsjConfig:
+        c = N.GsjConfig()
+        c.dim = n
+        c.indexed_dims = min(int(cfg.indexed_dims), n)
+        c.dtype = N.GSJ_FLOAT64 if dtype == np.float64 else N.GSJ_FLOAT32
+        c.reorder = int(cfg.reorder)
+        c.shortcircuit = int(cfg.shortcircuit)
+        c.ilp = int(cfg.ilp)
+        c.stamp = int(cfg.stamp)
+        c.query_reorder = int(cfg.query_reorder)
+        c.device = self.device
+        c.flags = N.GSJ_FLAG_QUIET | (N.GSJ_FLAG_SORT_LISTS if cfg.sort_lists else 0)
+        return c
+
+    def run(self, points, eps: float, config: JoinConfig | None = None, **kw) -> dict:
+        """Runs the join; returns the native statistics as a dict."""
+        cfg = config or JoinConfig(**kw)
+        st = N.GsjStats()
+        if hasattr(points, "is_cuda") and points.is_cuda:  # torch tensor on the device
+            import torch
+
+            if points.dim() != 2 or not points.is_contiguous():
+                raise ValueError("points must be a contiguous N x n tensor")
+            dt = np.float64 if points.dtype == torch.float64 else np.float32
+            if points.dtype not in (torch.float32, torch.float64):
+                raise TypeError("points must be float32 or float64")
+            Np, n = points.shape
+            c = self._cfg(n, dt, cfg)
+            N.check(self._L.gsj_join(self._ctx, ctypes.c_void_p(points.data_ptr()), Np, float(eps), ctypes.byref(c), 1,
+                                     ctypes.byref(st)), self._ctx)
+        else:
+            p = np.ascontiguousarray(points)
+            if p.dtype not in (np.float32, np.float64):
+                p = p.astype(np.float32)
+            if p.ndim != 2:
+                raise ValueError("points must be N x n")
+            Np, n = p.shape
+            c = self._cfg(n, p.dtype, cfg)
+            N.check(self._L.gsj_join(self._ctx, p.ctypes.data, Np, float(eps), ctypes.byref(c), 0, ctypes.byref(st)),
+                    self._ctx)
+        self.N, self.n = Np, n
+        return st.as_dict()
+
+    def total_pairs(self) -> int:
+        r = ctypes.c_uint64()
+        N.check(self._L.gsj_result_size(self._ctx, ctypes.byref(r)), self._ctx)
+        return int(r.value)
+
+    def counts(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty(self.N, dtype=np.uint32) if out is None else out
+        N.check(self._L.gsj_result_counts(self._ctx, out.ctypes.data, 0), self._ctx)
+        return out
+
+    def table(self, out: np.ndarray | None = None) -> np.ndarray:
+        R = self.total_pairs()
+        out = np.empty(R, dtype=np.uint32) if out is None else out
+        N.check(self._L.gsj_result_table(self._ctx, out.ctypes.data, out.size, 0), self._ctx)
+        return out
+
+    def counts_offsets_table_device(self):
+        """(counts int32[N], offsets int64[N+1], table int32[R]) as CUDA torch
+        tensors (copies of the context's result, device to device)."""
+        import torch
+
+        R = self.total_pairs()
+        dev = torch.device("cuda", self.device)
+        counts = torch.empty(self.N, dtype=torch.int32, device=dev)
+        table = torch.empty(max(R, 1), dtype=torch.int32, device=dev)[:R]
+        offsets = torch.empty(self.N + 1, dtype=torch.int64, device=dev)
+        cp, op, tp = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        N.check(self._L.gsj_result_device(self._ctx, ctypes.byref(cp), ctypes.byref(op), ctypes.byref(tp)), self._ctx)
+        N.check(self._L.gsj_result_counts(self._ctx, ctypes.c_void_p(counts.data_ptr()), 1), self._ctx)
+        if R:
+            N.check(self._L.gsj_result_table(self._ctx, ctypes.c_void_p(table.data_ptr()), R, 1), self._ctx)
+        torch.cuda.synchronize(dev)
+        # offsets: a device copy through a tensor view of the native buffer
+        offsets.copy_(torch.cumsum(torch.cat([torch.zeros(1, dtype=torch.int64, device=dev), counts.to(torch.int64)]),
+                                   0))
+        return counts, offsets, table
+
+
+def threshold(eps: float, dtype=np.float32) -> float:
+    """Largest s with sqrt(s) <= eps in dtype (the distance test's threshold)."""
+    L = N.lib()
+    if np.dtype(dtype) == np.float64:
+        return L.gsj_threshold_f64(float(eps))
+    return L.gsj_threshold_f32(float(eps))

@@ -1,0 +1,180 @@
+/*
+ * gpuselfjoin.h - C ABI of the B200 (sm_100a) epsilon-grid distance self-join.
+ *
+ * Drop-in for algorithm 3 of mgowanlock/gpu_self_join: every pair (q, c) of
+ * the N input points with sqrt(sum_l (c_l - q_l)^2) <= eps is reported (self
+ * pairs included), in the reference's own floating-point arithmetic, as one
+ * neighbour list per point:
+ *     numNeighbors[N]   (uint32)        - list length of point i
+ *     neighborTable[R]  (uint32)        - the lists, concatenated in point-id order
+ *
+ * The params.h switches of the reference become run-time fields of gsj_config
+ * (same names, same meaning).  All entry points return a status code (GSJ_OK
+ * == 0, negative on error) and never terminate the process; gsj_last_error()
+ * describes the most recent failure of the calling thread's default context.
+ *
+ * Plain C types only; no CUDA or PyTorch types appear in these signatures.
+ * Device pointers are passed as void* / uint32_t* and are marked as such.
+ */
+#ifndef GPUSELFJOIN_H
+#define GPUSELFJOIN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GSJ_API __attribute__((visibility("default")))
+#else
+#define GSJ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define GSJ_OK 0
+#define GSJ_ERR_INVALID (-1)    /* bad argument / configuration            */
+#define GSJ_ERR_CUDA (-2)       /* a CUDA runtime call failed              */
+#define GSJ_ERR_NOMEM (-3)      /* device or pinned host allocation failed */
+#define GSJ_ERR_STATE (-4)      /* call order violated (no result, ...)    */
+#define GSJ_ERR_OVERFLOW (-5)   /* a result count exceeds the ABI's range  */
+
+/* ---------------------------------------------------------------- dtype */
+#define GSJ_FLOAT32 0
+#define GSJ_FLOAT64 1
+
+/* flags */
+#define GSJ_FLAG_SORT_LISTS 0x1u  /* sort every neighbour list ascending       */
+#define GSJ_FLAG_QUIET      0x2u  /* no progress output on stdout              */
+
+/*
+ * Run-time configuration.  Field names follow params.h of the reference
+ * (params.h:17-93); the values have the same meaning.
+ */
+typedef struct gsj_config {
+    uint32_t dim;           /* GPUNUMDIM      number of dimensions n            */
+    uint32_t indexed_dims;  /* NUMINDEXEDDIM  grid dimensions k, 1 <= k <= n     */
+    uint32_t dtype;         /* DTYPE          GSJ_FLOAT32 or GSJ_FLOAT64         */
+    uint32_t reorder;       /* REORDER        permute dims by sampled variance   */
+    uint32_t shortcircuit;  /* SHORTCIRCUIT   early exit of the distance sum     */
+    uint32_t ilp;           /* ILP            accumulation order (0 = sequential)*/
+    uint32_t stamp;         /* STAMP          unidirectional cell comparison     */
+    uint32_t query_reorder; /* QUERYREORDER   schedule heavy query cells first   */
+    int32_t device;         /* gpuContext     CUDA device ordinal                */
+    uint32_t flags;         /* GSJ_FLAG_*                                        */
+} gsj_config;
+
+/* Statistics of the most recent join of a context. */
+typedef struct gsj_stats {
+    uint64_t num_points;      /* N                                              */
+    uint64_t total_pairs;     /* R = sum(numNeighbors)                          */
+    uint64_t candidates;      /* distance evaluations (reference COUNTMETRICS
+                                 workCounts[0] semantics for the traversal used)*/
+    uint64_t total_cells;     /* product of cells per indexed dim (main.cu:941) */
+    uint64_t nonempty_cells;  /* non-empty grid cells                           */
+    uint64_t work_items;      /* scheduled (query cell chunk) work items        */
+    double ms_h2d;            /* host->device copy of the dataset               */
+    double ms_index;          /* REORDER + grid extents + on-device index build */
+    double ms_join;           /* count pass + offsets + fill pass               */
+    double ms_d2h;            /* result copies to the host                      */
+    double ms_total;          /* whole call                                     */
+    /* device time (CUDA events on the context's stream) */
+    double dev_ms_index;      /* index build: keys, sort, cells, lookup, items  */
+    double dev_ms_count;      /* count pass kernel                              */
+    double dev_ms_fill;       /* fill pass kernel                               */
+    uint64_t kernel_launches; /* launches of this library's own kernels         */
+} gsj_stats;
+
+typedef struct gsj_context gsj_context;
+
+/* Fills *cfg with the build-time defaults (the GPUNUMDIM ... QUERYREORDER
+ * macros given when the library was built). */
+GSJ_API void gsj_default_config(gsj_config* cfg);
+
+/* Replaces the defaults used by GDSJoinPy (the run-time counterpart of
+ * rebuilding the reference with another params.h).  dim may be 0 (take NDIM). */
+GSJ_API int gsj_set_default_config(const gsj_config* cfg);
+
+/* Context: owns a CUDA stream and a device memory pool reused across joins. */
+GSJ_API int gsj_create(gsj_context** ctx, int device);
+GSJ_API int gsj_destroy(gsj_context* ctx);
+
+/*
+ * Runs the self-join.  `data` is a row-major N x cfg->dim array of cfg->dtype,
+ * in host memory (data_on_device == 0) or device memory of cfg->device
+ * (data_on_device == 1).  eps is converted to cfg->dtype first, as the
+ * reference stores epsilon as DTYPE (main.cu:98).  Results stay on the device
+ * until fetched with the gsj_result_* calls.  Replaces the mode-3 body of
+ * main.cu:178-262 and distanceTableNDGridBatches (GPU.cu:270-1088).
+ */
+GSJ_API int gsj_join(gsj_context* ctx, const void* data, uint64_t num_points, double eps,
+             const gsj_config* cfg, int data_on_device, gsj_stats* stats);
+
+/* Number of result pairs R of the last join. */
+GSJ_API int gsj_result_size(gsj_context* ctx, uint64_t* total_pairs);
+
+/* numNeighbors[N] of the last join, into host (dst_on_device == 0) or device
+ * memory.  storeNumberOfNeighborsForPython, main.cu:630-636. */
+GSJ_API int gsj_result_counts(gsj_context* ctx, uint32_t* num_neighbors, int dst_on_device);
+
+/* neighborTable[R] (capacity `cap` entries) into host or device memory; lists
+ * are concatenated in point-id order.  storeNeighborTableContiguousPython,
+ * main.cu:514-542.  Host destinations are filled through pinned staging
+ * buffers on two streams, overlapping the copy-out with the PCIe transfer. */
+GSJ_API int gsj_result_table(gsj_context* ctx, uint32_t* neighbor_table, uint64_t cap, int dst_on_device);
+
+/* Device pointers of the last result (valid until the next join or destroy):
+ * counts[N], offsets[N+1] (uint64 exclusive prefix), table[R]. */
+GSJ_API int gsj_result_device(gsj_context* ctx, const uint32_t** counts, const uint64_t** offsets,
+                      const uint32_t** table);
+
+/* Error text of the last failing call on ctx (or of the default context when
+ * ctx is NULL). */
+GSJ_API const char* gsj_last_error(gsj_context* ctx);
+
+/* The largest s with sqrt(s) <= eps in the given precision: the distance test
+ * sqrt(s) <= eps of kernel.cu:361/364 is evaluated as s <= threshold. */
+GSJ_API float gsj_threshold_f32(float eps);
+GSJ_API double gsj_threshold_f64(double eps);
+
+/* ---------------------------------------------------------------- drop-in
+ * The reference's shared-library ABI (built with -DPYTHON, Makefile:58-77).
+ *
+ * GDSJoinPy replaces main.cu:360 (`extern "C" void GDSJoinPy(DTYPE* dataset,
+ * unsigned int NUMPOINTS, DTYPE epsilon, unsigned int NDIM, int gpuContext,
+ * unsigned int* outNumNeighborsWithinEps)`).  DTYPE is float in the default
+ * build (define GSJ_DTYPE_DOUBLE at build time for double, as params.h:26
+ * does); the typed variants below take either precision.  The configuration is
+ * the build-time default (gsj_default_config) with dim = NDIM; when the library
+ * was built with a non-zero GPUNUMDIM, NDIM must equal it (main.cu:372-375).
+ * Unlike the reference, STAMP=1 is accepted and produces the same symmetric
+ * lists as STAMP=0, and nothing ever calls exit().
+ *
+ * copyResultIntoPythonArray replaces main.cu:507: it copies the first
+ * numResults entries of the table produced by the preceding GDSJoinPy and
+ * releases it.  The two calls are paired as in the reference; the pair is
+ * not re-entrant across threads.
+ */
+#ifdef GSJ_DTYPE_DOUBLE
+typedef double gsj_dtype_t;
+#else
+typedef float gsj_dtype_t;
+#endif
+GSJ_API void GDSJoinPy(gsj_dtype_t* dataset, unsigned int NUMPOINTS, gsj_dtype_t epsilon, unsigned int NDIM,
+               int gpuContext, unsigned int* outNumNeighborsWithinEps);
+GSJ_API void copyResultIntoPythonArray(unsigned int* outPythonNeighborTable, unsigned int numResults);
+
+/* Typed, status-returning forms of the same two calls.  The 64-bit count
+ * variant lifts the reference's 2^32 limit on the table size (main.cu:507). */
+GSJ_API int GDSJoinPy_f32(const float* dataset, unsigned int NUMPOINTS, float epsilon, unsigned int NDIM,
+                  int gpuContext, unsigned int* outNumNeighborsWithinEps);
+GSJ_API int GDSJoinPy_f64(const double* dataset, unsigned int NUMPOINTS, double epsilon, unsigned int NDIM,
+                  int gpuContext, unsigned int* outNumNeighborsWithinEps);
+GSJ_API int copyResultIntoPythonArray64(unsigned int* outPythonNeighborTable, uint64_t numResults);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUSELFJOIN_H */

@@ -1,0 +1,155 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle, which restates
+the reference's algorithm 3 with the reference's arithmetic.  Integer output:
+the per-point neighbour sets must be identical (bit-exact), compared as
+per-point sorted lists."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from gpu_self_join_b200 import JoinConfig, SelfJoin, gdsjoin, synth
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def canon(counts, table):
+    """Per-point lists sorted ascending (list order is not part of the output)."""
+    counts = np.asarray(counts, dtype=np.int64)
+    seg = np.repeat(np.arange(counts.size), counts)
+    return np.asarray(table)[np.lexsort((np.asarray(table), seg))]
+
+
+def run_gpu(points, eps, **kw):
+    with SelfJoin(0) as sj:
+        st = sj.run(points, eps, JoinConfig(**kw))
+        return sj.counts(), sj.table(), st
+
+
+def oracle_cfg(oracle, k, reorder=False, ilp=0, shortcircuit=False):
+    return oracle.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=shortcircuit)
+
+
+def assert_same(oracle, pts, eps, **kw):
+    k = min(kw.get("indexed_dims", 6), pts.shape[1])
+    ocfg = oracle_cfg(oracle, k, kw.get("reorder", False), kw.get("ilp", 0), kw.get("shortcircuit", False))
+    oc, _, on = oracle.join_lists(pts, eps, ocfg)
+    gc, gt, st = run_gpu(pts, eps, **kw)
+    assert gc.shape == oc.shape
+    assert np.array_equal(gc, oc), f"counts differ at {np.flatnonzero(gc != oc)[:10]}"
+    assert int(gc.sum(dtype=np.uint64)) == st["total_pairs"] == gt.size
+    assert np.array_equal(canon(gc, gt), on)
+    return st
+
+
+def test_readme_known_answer_through_gdsjoin():
+    pts = np.load(os.path.join(GOLD, "test_dat_f32.npy"))
+    with open(os.path.join(GOLD, "known_answers.json")) as f:
+        known = json.load(f)
+    num, table = gdsjoin(pts.reshape(-1).tolist(), 1.0, 2, "float")
+    assert int(num.sum(dtype=np.uint64)) == known["readme_known_answer"] == 27982028
+    from tests.golden.make_golden import lists_digest
+
+    assert lists_digest(num, canon(num, table)) == known["lists_sha256_device"]
+
+
+@pytest.mark.parametrize("stamp", [False, True])
+def test_c1_uniform_100k(oracle, stamp):
+    w = synth.WORKLOADS["c1_uniform2d"]
+    pts = synth.generate("c1_uniform2d")
+    st = assert_same(oracle, pts, w.eps, indexed_dims=2, stamp=stamp)
+    assert st["total_pairs"] > 3_000_000
+
+
+CASES = [
+    # n, k, dtype, reorder, ilp, sc, stamp, qr, N, eps
+    (2, 2, np.float64, False, 0, False, False, False, 20000, 1.0),
+    (3, 2, np.float32, False, 0, False, True, True, 20000, 1.5),
+    (4, 4, np.float64, False, 0, False, True, False, 20000, 2.5),
+    (5, 3, np.float64, True, 2, True, False, True, 20000, 2.0),
+    (6, 6, np.float32, False, 0, False, True, False, 30000, 3.0),
+    (7, 3, np.float32, True, 0, True, True, True, 20000, 2.5),
+    (8, 1, np.float32, False, 4, False, False, False, 5000, 2.0),
+    (18, 6, np.float32, True, 8, True, False, True, 20000, 4.0),
+    (18, 6, np.float32, True, 8, False, False, True, 20000, 4.0),
+    (18, 6, np.float32, False, 4, True, True, False, 20000, 4.0),
+    (90, 6, np.float32, True, 8, True, False, True, 5000, 12.0),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"n{c[0]}k{c[1]}{np.dtype(c[2]).name}r{int(c[3])}i{c[4]}s{int(c[5])}"
+                                             f"u{int(c[6])}q{int(c[7])}" for c in CASES])
+def test_configs_match_oracle(oracle, case):
+    n, k, dt, reorder, ilp, sc, stamp, qr, N, eps = case
+    rng = np.random.default_rng(1000 + n * 10 + k)
+    centres = rng.uniform(0, 20, size=(8, n))
+    pts = (centres[rng.integers(0, 8, N)] + rng.standard_normal((N, n)) * rng.uniform(0.5, 3, n)).astype(dt)
+    st = assert_same(oracle, pts, eps, indexed_dims=k, reorder=reorder, ilp=ilp, shortcircuit=sc, stamp=stamp,
+                     query_reorder=qr)
+    assert st["total_pairs"] > N  # more than the self pairs
+
+
+@pytest.mark.parametrize("stamp", [False, True])
+def test_dense_cell_many_chunks(oracle, stamp):
+    # 3000 points in few cells: query cells span many 32-query chunks
+    rng = np.random.default_rng(5)
+    pts = rng.uniform(0, 2.0, size=(3000, 2)).astype(np.float32)
+    assert_same(oracle, pts, 1.0, indexed_dims=2, stamp=stamp)
+
+
+def test_duplicates_and_eps_zero(oracle):
+    rng = np.random.default_rng(6)
+    base = rng.uniform(0, 50, size=(500, 3)).astype(np.float32)
+    pts = np.concatenate([base, base, base[:100]])
+    assert_same(oracle, pts, 1e-3, indexed_dims=3)
+    assert_same(oracle, pts, 2e-3, indexed_dims=3, stamp=True)
+
+
+def test_single_point_and_tiny():
+    c, t, st = run_gpu(np.array([[1.0, 2.0]], dtype=np.float32), 0.5, indexed_dims=2)
+    assert list(c) == [1] and list(t) == [0]
+    c, t, st = run_gpu(np.zeros((0, 2), dtype=np.float32), 0.5, indexed_dims=2)
+    assert c.size == 0 and t.size == 0
+
+
+def test_negative_and_offset_coordinates(oracle):
+    rng = np.random.default_rng(8)
+    pts = (rng.uniform(-500, -400, size=(20000, 2)) + np.float32(1.0e5)).astype(np.float32)
+    assert_same(oracle, pts, 0.8, indexed_dims=2, stamp=True)
+    pts2 = rng.uniform(-50, 50, size=(20000, 3)).astype(np.float32)
+    assert_same(oracle, pts2, 2.0, indexed_dims=2)
+
+
+def test_collinear_k1(oracle):
+    x = np.sort(np.random.default_rng(9).uniform(0, 1000, 30000)).astype(np.float32)
+    pts = np.stack([x, np.zeros_like(x)], 1)
+    assert_same(oracle, pts, 0.05, indexed_dims=1, stamp=True)
+
+
+def test_deterministic_without_stamp():
+    pts = synth.generate("c1_uniform2d")
+    c1, t1, _ = run_gpu(pts, 1.0, indexed_dims=2)
+    c2, t2, _ = run_gpu(pts, 1.0, indexed_dims=2)
+    assert np.array_equal(c1, c2) and np.array_equal(t1, t2)
+
+
+def test_large_properties():
+    """At 4M points of the 2-D mixture workload (too large for the oracle in a
+    test): lists are symmetric, contain the point itself, and the unicomp
+    traversal yields the same sets as the full traversal."""
+    w = synth.WORKLOADS["c2_gmm2d"]
+    pts = synth.generate("c2_gmm2d", 4_000_000)
+    eps = w.eps if w.eps > 0 else 0.5
+    c0, t0, s0 = run_gpu(pts, eps, indexed_dims=2, stamp=False)
+    c1, t1, s1 = run_gpu(pts, eps, indexed_dims=2, stamp=True)
+    assert np.array_equal(c0, c1)
+    assert np.array_equal(canon(c0, t0), canon(c1, t1))
+    seg = np.repeat(np.arange(c0.size, dtype=np.int64), c0.astype(np.int64))
+    q, c = seg, t0.astype(np.int64)
+    assert np.count_nonzero(q == c) == c0.size  # self pairs
+    fwd = np.sort(q * c0.size + c)
+    rev = np.sort(c * c0.size + q)
+    assert np.array_equal(fwd, rev)  # (q,c) present iff (c,q) present
+    assert s1["candidates"] < s0["candidates"]
