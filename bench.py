@@ -59,21 +59,18 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines: list[str] = []
-        self.t = None
+        self.path = None
 
     def start(self):
+        import tempfile
+
+        self.path = tempfile.mktemp(suffix=".csv")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+                                          "--format=csv,noheader,nounits", "-lms", "100", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-
-    def _read(self):
-        for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -83,6 +80,12 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        try:
+            with open(self.path) as f:
+                self.lines = [ln.strip() for ln in f]
+            os.remove(self.path)
+        except OSError:
+            self.lines = []
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
@@ -166,7 +169,7 @@ def _ours(args) -> None:
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     w = synth.WORKLOADS[args.workload]
-    pts = synth.generate(args.workload)
+    pts = synth.generate(args.workload, args.points)
     N, n = pts.shape
     cfg = JoinConfig(indexed_dims=w.k, reorder=w.reorder, shortcircuit=w.shortcircuit, ilp=w.ilp, stamp=w.stamp,
                      query_reorder=w.query_reorder)
@@ -335,10 +338,12 @@ def _run_rtree_harness(harness, pts, w, cores, seed):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2_gmm2d")
+    ap.add_argument("--points", type=int, default=None,
+                    help="generate a smaller instance of the workload (profiling captures only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

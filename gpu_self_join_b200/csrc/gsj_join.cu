@@ -77,64 +77,115 @@ __device__ __forceinline__ int lookup_cell(const JoinArgs<T>& a, uint64_t lin) {
     return -1;
 }
 
+// Contraction policy of the reference's device arithmetic.  The source
+// accumulates `acc += d*d` from acc = 0; nvcc turns it into fused
+// multiply-adds in a precision-dependent way, pinned against the reference's
+// own builds:
+//   kPolF32     0 + d*d stays fma(d, d, 0): every later term is fused into
+//               the accumulator (float).
+//   kPolF64Seq  0 + d*d folds to a pending product; when an addition has two
+//               pending products the accumulator's product is fused
+//               (double, sequential loop).
+//   kPolF64Ilp  as kPolF64Seq, but the added term's product is fused (double,
+//               ILP loops).
+enum Policy : int { kPolF32 = 0, kPolF64Seq = 1, kPolF64Ilp = 2 };
+
+template <typename T, int POL>
+struct Acc {
+    static constexpr bool FOLD0 = POL != kPolF32;
+    static constexpr bool LEFT = POL == kPolF64Seq;
+    T v, d;
+    int st;  // 0: literal zero, 1: pending product d*d (value v), 2: value v
+    __device__ __forceinline__ Acc() : v(T(0)), d(T(0)), st(0) {}
+    __device__ __forceinline__ void add_prod(T dd) {
+        if (st == 0) {
+            if (FOLD0) {
+                st = 1;
+                d = dd;
+                v = FP<T>::mul(dd, dd);
+            } else {
+                st = 2;
+                v = FP<T>::fma(dd, dd, T(0));
+            }
+        } else if (FOLD0 && st == 1) {
+            st = 2;
+            v = LEFT ? FP<T>::fma(d, d, FP<T>::mul(dd, dd)) : FP<T>::fma(dd, dd, v);
+        } else {
+            v = FP<T>::fma(dd, dd, v);
+        }
+    }
+    __device__ __forceinline__ void add_acc(const Acc& o) {
+        if (o.st == 0) return;
+        if (st == 0) {
+            *this = o;
+            return;
+        }
+        if (FOLD0 && st == 1 && o.st == 1) {
+            v = LEFT ? FP<T>::fma(d, d, o.v) : FP<T>::fma(o.d, o.d, v);
+        } else if (FOLD0 && o.st == 1) {
+            v = FP<T>::fma(o.d, o.d, v);
+        } else if (FOLD0 && st == 1) {
+            v = FP<T>::fma(d, d, o.v);
+        } else {
+            v = FP<T>::add(v, o.v);
+        }
+        st = 2;
+    }
+};
+
 // Squared distance in the reference's order with the candidate row in
 // registers (NT = n known at compile time; sequential model only).
-template <typename T, int NT>
+template <typename T, int NT, int POL>
 __device__ __forceinline__ T sqdist_seq_reg(const T* __restrict__ q, const T (&c)[NT]) {
-    T s = T(0);
+    Acc<T, POL> s;
 #pragma unroll
-    for (int l = 0; l < NT; l++) {
-        const T d = FP<T>::sub(c[l], q[l]);
-        s = FP<T>::fma(d, d, s);
-    }
-    return s;
+    for (int l = 0; l < NT; l++) s.add_prod(FP<T>::sub(c[l], q[l]));
+    return s.v;
 }
 
-// Generic n: candidate row and query row in shared memory.  `alive` is the
+// Generic n: candidate row and query row in shared memory.  `valid` is the
 // lane's vote input for the warp-wide early exit; an exit never changes a
 // decision because every model's running sum only grows once it is above thr.
-template <typename T, int MODEL>
+template <typename T, int MODEL, int POL>
 __device__ __forceinline__ T sqdist_generic(const T* __restrict__ q, const T* __restrict__ c, uint32_t n,
                                             uint32_t ilp, T thr, bool valid) {
     const unsigned FULL = 0xffffffffu;
     if (MODEL == kSeq) {
-        T s = T(0);
+        // kernel.cu:346-356
+        Acc<T, POL> s;
         for (uint32_t l = 0; l < n; l++) {
-            const T d = FP<T>::sub(c[l], q[l]);
-            s = FP<T>::fma(d, d, s);
-            if ((l & 7u) == 7u && __all_sync(FULL, !valid || s > thr)) break;
+            s.add_prod(FP<T>::sub(c[l], q[l]));
+            if ((l & 7u) == 7u && __all_sync(FULL, !valid || s.v > thr)) break;
         }
-        return s;
+        return s.v;
     } else if (MODEL == kIlp) {
         // runningDist[j] accumulates dims l == j (mod ILP); then summed in j order (kernel.cu:312-341)
-        T s = T(0);
+        Acc<T, POL> s;
         for (uint32_t j = 0; j < ilp; j++) {
-            T r = T(0);
-            for (uint32_t l = j; l < n; l += ilp) {
-                const T d = FP<T>::sub(c[l], q[l]);
-                r = FP<T>::fma(d, d, r);
-            }
-            s = (j == 0) ? r : FP<T>::add(s, r);
+            Acc<T, POL> r;
+            for (uint32_t l = j; l < n; l += ilp) r.add_prod(FP<T>::sub(c[l], q[l]));
+            if (j == 0) s = r;
+            else s.add_acc(r);
         }
-        return s;
+        return s.v;
     } else {
-        // SHORTCIRCUIT with ILP: per block, the first dim is fused into the
-        // running total, the others are squared separately and added in order.
-        T s = T(0);
+        // SHORTCIRCUIT with ILP (kernel.cu:320-334): per block, runningDist[0]
+        // takes the block's first square, then the other registers are added.
+        Acc<T, POL> r0;
         for (uint32_t l = 0; l < n; l += ilp) {
-            T d = FP<T>::sub(c[l], q[l]);
-            s = FP<T>::fma(d, d, s);
+            r0.add_prod(FP<T>::sub(c[l], q[l]));
             for (uint32_t j = 1; j < ilp && l + j < n; j++) {
-                d = FP<T>::sub(c[l + j], q[l + j]);
-                s = FP<T>::add(s, FP<T>::mul(d, d));
+                Acc<T, POL> rj;
+                rj.add_prod(FP<T>::sub(c[l + j], q[l + j]));
+                r0.add_acc(rj);
             }
-            if (__all_sync(FULL, !valid || s > thr)) break;
+            if (__all_sync(FULL, !valid || r0.v > thr)) break;
         }
-        return s;
+        return r0.v;
     }
 }
 
-template <typename T, int NT, int MODEL, bool STAMP, int PASS>
+template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS>
 __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool GENERIC = (NT == 0);
@@ -265,9 +316,9 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                 const T* q = q_s + (size_t)j * npad;
                 T s;
                 if (!GENERIC) {
-                    if constexpr (NT > 0) s = sqdist_seq_reg<T, NT>(q, creg);
+                    if constexpr (NT > 0) s = sqdist_seq_reg<T, NT, POL>(q, creg);
                 } else {
-                    s = sqdist_generic<T, MODEL>(q, cand_s + (size_t)lane * (npad + 1u), a.n, a.ilp, a.thr, valid);
+                    s = sqdist_generic<T, MODEL, POL>(q, cand_s + (size_t)lane * (npad + 1u), a.n, a.ilp, a.thr, valid);
                 }
                 const bool hit = valid && (s <= a.thr);
                 const unsigned b = __ballot_sync(FULL, hit);
@@ -306,9 +357,9 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
 }
 
 // ------------------------------------------------------------------ launch
-template <typename T, int NT, int MODEL, bool STAMP, int PASS>
+template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS>
 static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, int num_sms, cudaStream_t st) {
-    auto kern = k_join<T, NT, MODEL, STAMP, PASS>;
+    auto kern = k_join<T, NT, MODEL, POL, STAMP, PASS>;
     const WarpSmem L = warp_smem_layout(a.npad, sizeof(T), nb_cap, NT == 0);
     const uint32_t max_smem = 200u * 1024u;
     int warps = (int)(max_smem / L.total);
@@ -329,28 +380,33 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     return cudaGetLastError();
 }
 
-template <typename T, int MODEL, bool STAMP, int PASS>
+template <typename T, int MODEL, int POL, bool STAMP, int PASS>
 static cudaError_t dispatch_nt(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, int num_sms, cudaStream_t st) {
     if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
         switch (a.n) {
-            case 2: return launch_one<T, 2, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 3: return launch_one<T, 3, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 4: return launch_one<T, 4, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 6: return launch_one<T, 6, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 8: return launch_one<T, 8, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 2: return launch_one<T, 2, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 3: return launch_one<T, 3, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 4: return launch_one<T, 4, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 6: return launch_one<T, 6, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 8: return launch_one<T, 8, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
             default: break;
         }
     }
-    return launch_one<T, 0, MODEL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+    return launch_one<T, 0, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
 }
 
+// float32 keeps one policy; float64 uses the sequential-loop policy without
+// ILP and the ILP-loop policy with it.
 template <typename T, bool STAMP, int PASS>
 static cudaError_t dispatch_model(const JoinArgs<T>& a, int model, uint32_t nb_cap, uint32_t noff, int num_sms,
                                   cudaStream_t st) {
+    constexpr bool F64 = sizeof(T) == 8;
+    constexpr int PS = F64 ? kPolF64Seq : kPolF32;
+    constexpr int PI = F64 ? kPolF64Ilp : kPolF32;
     switch (model) {
-        case kSeq: return dispatch_nt<T, kSeq, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-        case kIlp: return dispatch_nt<T, kIlp, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-        case kIlpSc: return dispatch_nt<T, kIlpSc, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kSeq: return dispatch_nt<T, kSeq, PS, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kIlp: return dispatch_nt<T, kIlp, PI, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kIlpSc: return dispatch_nt<T, kIlpSc, PI, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
         default: return cudaErrorInvalidValue;
     }
 }

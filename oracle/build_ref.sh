@@ -34,6 +34,13 @@ CONFIGS=(
   "d18_k6_ilp4_sc 18  6 float  0 1 4 1 0 1"
   "d90_k6_ilp8_sc 90  6 float  0 1 8 1 1 1"
   "d5_k3_f64_ilp2_sc 5 3 double 0 1 2 1 1 1"
+  "d5_k3_f64_plain   5 3 double 0 1 0 0 0 1"
+  "d18_k6_f64_ilp8  18 6 double 0 1 8 0 1 1"
+  "d18_k6_f64_ilp8_sc 18 6 double 0 1 8 1 1 1"
+  "d5_k3_f32_ilp8    5 3 float  0 1 8 0 0 1"
+  "d5_k3_f64_ilp8    5 3 double 0 1 8 0 0 1"
+  "d3_k3_f64_ilp2    3 3 double 0 0 2 0 0 1"
+  "d5_k3_f32_ilp2_sc 5 3 float  0 1 2 1 1 1"
 )
 
 write_params() {  # $1 dir, then the fields

@@ -52,11 +52,13 @@ struct orc_cfg {
     uint32_t ilp;          // ILP (0 = sequential accumulation)
     uint32_t shortcircuit; // SHORTCIRCUIT
     uint32_t model;        // MODEL_*
-    uint32_t sc_contract;  // ILP>0 && SC: contract the cross-register adds too
+    uint32_t sc_contract;  // alias of fold_zero = 1, fuse_left = 0 (kept for callers)
     uint32_t stamp_ref;    // 1: emit the reference's STAMP=1 output (duplicated
                            //    (q,c) pairs, kernel.cu:367-375) instead of the
                            //    symmetric neighbour lists
     uint32_t nthreads;     // OpenMP threads (0 = default)
+    uint32_t fold_zero;    // device contraction policy, see DevNode
+    uint32_t fuse_left;
 };
 
 }  // extern "C"
@@ -77,6 +79,43 @@ template <>
 inline float sqrtT<float>(float x) { return sqrtf(x); }
 template <>
 inline double sqrtT<double>(double x) { return sqrt(x); }
+
+// A value of the device-side distance expression.  The reference accumulates
+// `acc += d*d` from acc = 0; how nvcc turns that source into fused
+// multiply-adds depends on the precision, and is pinned against the
+// reference's own builds (tests/golden/ref_pins.json):
+//   * a product d*d is "pending" until it is added to something;
+//   * acc + pending            -> fma(d, d, acc)              (contraction)
+//   * 0 + pending              -> fma(d, d, 0) = round(d*d)   (fold_zero = 0)
+//                                 or stays pending            (fold_zero = 1)
+//   * pending + pending        -> fma(d_l, d_l, round(d_r*d_r)) (fuse_left = 1)
+//                                 or fma(d_r, d_r, round(d_l*d_l)) (fuse_left = 0)
+//   * value + value            -> plain rounded addition.
+template <typename T>
+struct DevNode {
+    T v;         // rounded value
+    T d;         // the difference whose square is pending (prod only)
+    bool is_prod;  // pending product d*d
+    bool is_zero;  // the literal 0 the accumulators start from
+    static DevNode make_zero() { return {T(0), T(0), false, true}; }
+    static DevNode make_prod(T d) { return {d * d, d, true, false}; }
+};
+
+template <typename T>
+DevNode<T> dev_add(const DevNode<T>& x, const DevNode<T>& y, bool fold0, bool left) {
+    if (y.is_zero) return x;
+    if (x.is_zero) {
+        if (y.is_prod && !fold0) return {fmaT<T>(y.d, y.d, T(0)), T(0), false, false};
+        return y;
+    }
+    if (x.is_prod && y.is_prod) {
+        if (left) return {fmaT<T>(x.d, x.d, y.v), T(0), false, false};
+        return {fmaT<T>(y.d, y.d, x.v), T(0), false, false};
+    }
+    if (y.is_prod) return {fmaT<T>(y.d, y.d, x.v), T(0), false, false};
+    if (x.is_prod) return {fmaT<T>(x.d, x.d, y.v), T(0), false, false};
+    return {x.v + y.v, T(0), false, false};
+}
 
 // Returns true when point c is within eps of point p under the configured model.
 // p is the query ("point" in kernel.cu:307), c the candidate ("database[dataIdx]").
@@ -100,42 +139,36 @@ bool within(const T* p, const T* c, uint32_t n, T eps, const orc_cfg& cfg) {
         }
         return sqrtT<T>(s) <= eps;
     }
-    // MODEL_DEVICE
+    // MODEL_DEVICE: the source-level expression of kernel.cu:312-365 evaluated
+    // under the compiler's contraction policy (see DevNode).
     const uint32_t ilp = cfg.ilp;
+    const bool fold0 = cfg.sc_contract || cfg.fold_zero;
+    const bool left = cfg.fuse_left;
+    auto P = [&](uint32_t l) { return DevNode<T>::make_prod(c[l] - p[l]); };
     if (ilp == 0) {
-        // kernel.cu:346-356: runningTotalDist += d*d  ->  fma(d, d, s)
-        T s = 0;
+        // kernel.cu:346-356: runningTotalDist += d*d
+        DevNode<T> s = DevNode<T>::make_zero();
         for (uint32_t l = 0; l < n; l++) {
-            T d = c[l] - p[l];
-            s = fmaT<T>(d, d, s);
-            if (cfg.shortcircuit && sqrtT<T>(s) > eps) return false;  // kernel.cu:350-353
+            s = dev_add(s, P(l), fold0, left);
+            if (cfg.shortcircuit && sqrtT<T>(s.v) > eps) return false;  // kernel.cu:350-353
         }
-        return sqrtT<T>(s) <= eps;
+        return sqrtT<T>(s.v) <= eps;
     }
     // kernel.cu:312-341: ILP accumulators runningDist[0..ILP-1]
-    T r[64];
-    for (uint32_t j = 0; j < ilp; j++) r[j] = 0;
+    DevNode<T> r[64];
+    for (uint32_t j = 0; j < ilp; j++) r[j] = DevNode<T>::make_zero();
     for (uint32_t l = 0; l < n; l += ilp) {
-        for (uint32_t j = 0; j < ilp && (l + j) < n; j++) {
-            T d = c[l + j] - p[l + j];
-            if (cfg.shortcircuit && j > 0 && cfg.sc_contract) {
-                // variant: the compiler folds r[j] (known 0 here) away and
-                // contracts r[0] += d*d into one fma.
-                r[0] = fmaT<T>(d, d, r[0]);
-            } else {
-                r[j] = fmaT<T>(d, d, r[j]);
-            }
-        }
+        for (uint32_t j = 0; j < ilp && (l + j) < n; j++) r[j] = dev_add(r[j], P(l + j), fold0, left);
         if (cfg.shortcircuit) {
             for (uint32_t j = 1; j < ilp; j++) {
-                if (!cfg.sc_contract) r[0] = r[0] + r[j];
-                r[j] = 0;
+                r[0] = dev_add(r[0], r[j], fold0, left);
+                r[j] = DevNode<T>::make_zero();
             }
-            if (sqrtT<T>(r[0]) > eps) return false;  // kernel.cu:331-333
+            if (sqrtT<T>(r[0].v) > eps) return false;  // kernel.cu:331-333
         }
     }
-    for (uint32_t j = 1; j < ilp; j++) r[0] = r[0] + r[j];  // kernel.cu:337-340
-    return sqrtT<T>(r[0]) <= eps;
+    for (uint32_t j = 1; j < ilp; j++) r[0] = dev_add(r[0], r[j], fold0, left);  // kernel.cu:337-340
+    return sqrtT<T>(r[0].v) <= eps;
 }
 
 // ---------------------------------------------------------------- REORDER

@@ -34,6 +34,8 @@ class _Cfg(ctypes.Structure):
         ("sc_contract", ctypes.c_uint32),
         ("stamp_ref", ctypes.c_uint32),
         ("nthreads", ctypes.c_uint32),
+        ("fold_zero", ctypes.c_uint32),
+        ("fuse_left", ctypes.c_uint32),
     ]
 
 
@@ -49,10 +51,26 @@ class OracleConfig:
     sc_contract: bool = False
     stamp_ref: bool = False   # reproduce the reference's STAMP=1 duplicated output
     nthreads: int = 0
+    fold_zero: bool | None = None  # None: the pinned policy of the dtype
+    fuse_left: bool | None = None
 
-    def c(self) -> _Cfg:
+    def c(self, dtype=np.float32) -> _Cfg:
+        fz, fl = pinned_policy(dtype, self.ilp)
+        fz = fz if self.fold_zero is None else self.fold_zero
+        fl = fl if self.fuse_left is None else self.fuse_left
         return _Cfg(self.k, int(self.reorder), self.ilp, int(self.shortcircuit), self.model,
-                    int(self.sc_contract), int(self.stamp_ref), self.nthreads)
+                    int(self.sc_contract), int(self.stamp_ref), self.nthreads, int(fz), int(fl))
+
+
+def pinned_policy(dtype, ilp: int = 0) -> tuple[bool, bool]:
+    """(fold_zero, fuse_left) of the reference's device arithmetic, as pinned
+    against the reference's own builds (tests/golden/ref_pins.json): float32
+    keeps fma(d, d, 0); float64 folds it to a pending product and, when both
+    operands of an addition are pending products, fuses the accumulator's
+    in the sequential loop and the added term's in the ILP loop."""
+    if np.dtype(dtype) == np.float64:
+        return True, ilp == 0
+    return False, False
 
 
 _lib = None
@@ -108,7 +126,7 @@ def join_counts(points: np.ndarray, eps: float, cfg: OracleConfig):
     counts = np.zeros(N, dtype=np.uint32)
     total = ctypes.c_uint64()
     cand = ctypes.c_uint64()
-    c = cfg.c()
+    c = cfg.c(p.dtype)
     rc = getattr(lib(), f"orc_join_counts_{s}")(p.ctypes.data, N, n, eps, ctypes.byref(c),
                                                 counts.ctypes.data, ctypes.byref(total),
                                                 ctypes.byref(cand))
@@ -126,7 +144,7 @@ def join_lists(points: np.ndarray, eps: float, cfg: OracleConfig):
     offsets = np.zeros(N + 1, dtype=np.uint64)
     np.cumsum(counts, out=offsets[1:])
     nbrs = np.zeros(total, dtype=np.uint32)
-    c = cfg.c()
+    c = cfg.c(p.dtype)
     rc = getattr(lib(), f"orc_join_lists_{_sfx(p)}")(p.ctypes.data, N, n, eps, ctypes.byref(c),
                                                      offsets.ctypes.data, nbrs.ctypes.data)
     if rc != 0:
@@ -139,7 +157,7 @@ def bruteforce_counts(points: np.ndarray, eps: float, cfg: OracleConfig):
     N, n = p.shape
     counts = np.zeros(N, dtype=np.uint32)
     total = ctypes.c_uint64()
-    c = cfg.c()
+    c = cfg.c(p.dtype)
     getattr(lib(), f"orc_bruteforce_counts_{_sfx(p)}")(p.ctypes.data, N, n, eps, ctypes.byref(c),
                                                        counts.ctypes.data, ctypes.byref(total))
     return counts, int(total.value)
@@ -170,7 +188,7 @@ def grid_dims(points: np.ndarray, k: int, eps: float):
 def within(p: np.ndarray, c: np.ndarray, eps: float, cfg: OracleConfig) -> bool:
     p = np.ascontiguousarray(p)
     c = np.ascontiguousarray(c, dtype=p.dtype)
-    cc = cfg.c()
+    cc = cfg.c(p.dtype)
     return bool(getattr(lib(), f"orc_within_{_sfx(p)}")(p.ctypes.data, c.ctypes.data, p.shape[0],
                                                         eps, ctypes.byref(cc)))
 
@@ -199,7 +217,7 @@ def ref_batch_plan(points: np.ndarray, eps: float, cfg: OracleConfig, ref_counts
     nb = ctypes.c_uint32()
     bs = ctypes.c_uint32()
     mx = ctypes.c_uint64()
-    c = cfg.c()
+    c = cfg.c(np.float32)
     lib().orc_ref_batch_plan_f32(p.ctypes.data, N, n, eps, ctypes.byref(c), rc.ctypes.data,
                                  sc.ctypes.data, int(query_reorder), alpha, ctypes.byref(est),
                                  ctypes.byref(nb), ctypes.byref(bs), ctypes.byref(mx))
@@ -214,7 +232,7 @@ def join_sample(points: np.ndarray, eps: float, cfg: OracleConfig, queries: np.n
     tot = ctypes.c_uint64()
     si = ctypes.c_double()
     sq = ctypes.c_double()
-    c = cfg.c()
+    c = cfg.c(np.float32)
     lib().orc_join_sample_f32(p.ctypes.data, N, n, eps, ctypes.byref(c), q.ctypes.data, q.size, ctypes.byref(tot),
                               ctypes.byref(si), ctypes.byref(sq))
     return int(tot.value), float(si.value), float(sq.value)

@@ -46,6 +46,13 @@ PIN_CONFIGS = {
     "d18_k6_ilp4_sc": (18, 6, "float32", True, 4, True, False, 30000, 3.0),
     "d90_k6_ilp8_sc": (90, 6, "float32", True, 8, True, True, 8000, 8.0),
     "d5_k3_f64_ilp2_sc": (5, 3, "float64", True, 2, True, True, 30000, 2.0),
+    "d5_k3_f64_plain": (5, 3, "float64", True, 0, False, False, 30000, 2.0),
+    "d18_k6_f64_ilp8": (18, 6, "float64", True, 8, False, True, 30000, 3.0),
+    "d18_k6_f64_ilp8_sc": (18, 6, "float64", True, 8, True, True, 30000, 3.0),
+    "d5_k3_f32_ilp8": (5, 3, "float32", True, 8, False, False, 30000, 2.0),
+    "d5_k3_f64_ilp8": (5, 3, "float64", True, 8, False, False, 30000, 2.0),
+    "d3_k3_f64_ilp2": (3, 3, "float64", False, 2, False, False, 30000, 2.0),
+    "d5_k3_f32_ilp2_sc": (5, 3, "float32", True, 2, True, True, 30000, 2.0),
 }
 
 
@@ -88,10 +95,15 @@ def parse_dssj(path: str, N: int):
 
 
 def oracle_variants(O, name, pts):
+    """Every contraction policy of the device model (see DevNode in
+    oracle/gsj_oracle.cpp) plus the host's unfused arithmetic."""
     n, k, dt, reorder, ilp, sc, qr, N, eps = PIN_CONFIGS[name]
-    out = {"fused": O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc)}
-    if ilp and sc:
-        out["fused_contracted_sc"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc, sc_contract=True)
+    out = {}
+    for fz in (False, True):
+        for fl in (False, True):
+            out[f"fold{int(fz)}_left{int(fl)}"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc,
+                                                                 fold_zero=fz, fuse_left=fl)
+    out["pinned"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc)
     out["host_unfused"] = O.OracleConfig(k=k, reorder=reorder, ilp=0, model=O.MODEL_HOST)
     return out
 

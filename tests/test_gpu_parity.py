@@ -75,7 +75,7 @@ CASES = [
     (18, 6, np.float32, True, 8, True, False, True, 20000, 4.0),
     (18, 6, np.float32, True, 8, False, False, True, 20000, 4.0),
     (18, 6, np.float32, False, 4, True, True, False, 20000, 4.0),
-    (90, 6, np.float32, True, 8, True, False, True, 5000, 12.0),
+    (90, 6, np.float32, True, 8, True, False, True, 5000, 20.0),
 ]
 
 
