@@ -27,6 +27,7 @@
 
 #include "gsj_common.cuh"
 #include "gsj_fp.cuh"
+#include "gsj_dist.cuh"
 #include "gsj_kernels.h"
 
 namespace gsj {
@@ -75,114 +76,6 @@ __device__ __forceinline__ int lookup_cell(const JoinArgs<T>& a, uint64_t lin) {
         h = (h + 1) & a.hmask;
     }
     return -1;
-}
-
-// Contraction policy of the reference's device arithmetic.  The source
-// accumulates `acc += d*d` from acc = 0; nvcc turns it into fused
-// multiply-adds in a precision-dependent way, pinned against the reference's
-// own builds:
-//   kPolF32     0 + d*d stays fma(d, d, 0): every later term is fused into
-//               the accumulator (float).
-//   kPolF64Seq  0 + d*d folds to a pending product; when an addition has two
-//               pending products the accumulator's product is fused
-//               (double, sequential loop).
-//   kPolF64Ilp  as kPolF64Seq, but the added term's product is fused (double,
-//               ILP loops).
-enum Policy : int { kPolF32 = 0, kPolF64Seq = 1, kPolF64Ilp = 2 };
-
-template <typename T, int POL>
-struct Acc {
-    static constexpr bool FOLD0 = POL != kPolF32;
-    static constexpr bool LEFT = POL == kPolF64Seq;
-    T v, d;
-    int st;  // 0: literal zero, 1: pending product d*d (value v), 2: value v
-    __device__ __forceinline__ Acc() : v(T(0)), d(T(0)), st(0) {}
-    __device__ __forceinline__ void add_prod(T dd) {
-        if (st == 0) {
-            if (FOLD0) {
-                st = 1;
-                d = dd;
-                v = FP<T>::mul(dd, dd);
-            } else {
-                st = 2;
-                v = FP<T>::fma(dd, dd, T(0));
-            }
-        } else if (FOLD0 && st == 1) {
-            st = 2;
-            v = LEFT ? FP<T>::fma(d, d, FP<T>::mul(dd, dd)) : FP<T>::fma(dd, dd, v);
-        } else {
-            v = FP<T>::fma(dd, dd, v);
-        }
-    }
-    __device__ __forceinline__ void add_acc(const Acc& o) {
-        if (o.st == 0) return;
-        if (st == 0) {
-            *this = o;
-            return;
-        }
-        if (FOLD0 && st == 1 && o.st == 1) {
-            v = LEFT ? FP<T>::fma(d, d, o.v) : FP<T>::fma(o.d, o.d, v);
-        } else if (FOLD0 && o.st == 1) {
-            v = FP<T>::fma(o.d, o.d, v);
-        } else if (FOLD0 && st == 1) {
-            v = FP<T>::fma(d, d, o.v);
-        } else {
-            v = FP<T>::add(v, o.v);
-        }
-        st = 2;
-    }
-};
-
-// Squared distance in the reference's order with the candidate row in
-// registers (NT = n known at compile time; sequential model only).
-template <typename T, int NT, int POL>
-__device__ __forceinline__ T sqdist_seq_reg(const T* __restrict__ q, const T (&c)[NT]) {
-    Acc<T, POL> s;
-#pragma unroll
-    for (int l = 0; l < NT; l++) s.add_prod(FP<T>::sub(c[l], q[l]));
-    return s.v;
-}
-
-// Generic n: candidate row and query row in shared memory.  `valid` is the
-// lane's vote input for the warp-wide early exit; an exit never changes a
-// decision because every model's running sum only grows once it is above thr.
-template <typename T, int MODEL, int POL>
-__device__ __forceinline__ T sqdist_generic(const T* __restrict__ q, const T* __restrict__ c, uint32_t n,
-                                            uint32_t ilp, T thr, bool valid) {
-    const unsigned FULL = 0xffffffffu;
-    if (MODEL == kSeq) {
-        // kernel.cu:346-356
-        Acc<T, POL> s;
-        for (uint32_t l = 0; l < n; l++) {
-            s.add_prod(FP<T>::sub(c[l], q[l]));
-            if ((l & 7u) == 7u && __all_sync(FULL, !valid || s.v > thr)) break;
-        }
-        return s.v;
-    } else if (MODEL == kIlp) {
-        // runningDist[j] accumulates dims l == j (mod ILP); then summed in j order (kernel.cu:312-341)
-        Acc<T, POL> s;
-        for (uint32_t j = 0; j < ilp; j++) {
-            Acc<T, POL> r;
-            for (uint32_t l = j; l < n; l += ilp) r.add_prod(FP<T>::sub(c[l], q[l]));
-            if (j == 0) s = r;
-            else s.add_acc(r);
-        }
-        return s.v;
-    } else {
-        // SHORTCIRCUIT with ILP (kernel.cu:320-334): per block, runningDist[0]
-        // takes the block's first square, then the other registers are added.
-        Acc<T, POL> r0;
-        for (uint32_t l = 0; l < n; l += ilp) {
-            r0.add_prod(FP<T>::sub(c[l], q[l]));
-            for (uint32_t j = 1; j < ilp && l + j < n; j++) {
-                Acc<T, POL> rj;
-                rj.add_prod(FP<T>::sub(c[l + j], q[l + j]));
-                r0.add_acc(rj);
-            }
-            if (__all_sync(FULL, !valid || r0.v > thr)) break;
-        }
-        return r0.v;
-    }
 }
 
 template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS>
@@ -395,18 +288,14 @@ static cudaError_t dispatch_nt(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t n
     return launch_one<T, 0, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
 }
 
-// float32 keeps one policy; float64 uses the sequential-loop policy without
-// ILP and the ILP-loop policy with it.
 template <typename T, bool STAMP, int PASS>
 static cudaError_t dispatch_model(const JoinArgs<T>& a, int model, uint32_t nb_cap, uint32_t noff, int num_sms,
                                   cudaStream_t st) {
-    constexpr bool F64 = sizeof(T) == 8;
-    constexpr int PS = F64 ? kPolF64Seq : kPolF32;
-    constexpr int PI = F64 ? kPolF64Ilp : kPolF32;
+    constexpr int P = sizeof(T) == 8 ? kPolF64 : kPolF32;
     switch (model) {
-        case kSeq: return dispatch_nt<T, kSeq, PS, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-        case kIlp: return dispatch_nt<T, kIlp, PI, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-        case kIlpSc: return dispatch_nt<T, kIlpSc, PI, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kSeq: return dispatch_nt<T, kSeq, P, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kIlp: return dispatch_nt<T, kIlp, P, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kIlpSc: return dispatch_nt<T, kIlpSc, P, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
         default: return cudaErrorInvalidValue;
     }
 }

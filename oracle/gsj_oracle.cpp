@@ -58,7 +58,8 @@ struct orc_cfg {
                            //    symmetric neighbour lists
     uint32_t nthreads;     // OpenMP threads (0 = default)
     uint32_t fold_zero;    // device contraction policy, see DevNode
-    uint32_t fuse_left;
+    uint32_t fuse_left;    // chains acc += d*d
+    uint32_t cross_left;   // cross-register sums runningDist[0] += runningDist[j]
 };
 
 }  // extern "C"
@@ -88,8 +89,10 @@ inline double sqrtT<double>(double x) { return sqrt(x); }
 //   * acc + pending            -> fma(d, d, acc)              (contraction)
 //   * 0 + pending              -> fma(d, d, 0) = round(d*d)   (fold_zero = 0)
 //                                 or stays pending            (fold_zero = 1)
-//   * pending + pending        -> fma(d_l, d_l, round(d_r*d_r)) (fuse_left = 1)
-//                                 or fma(d_r, d_r, round(d_l*d_l)) (fuse_left = 0)
+//   * pending + pending        -> fma(d_l, d_l, round(d_r*d_r)) (left)
+//                                 or fma(d_r, d_r, round(d_l*d_l)) (right);
+//                                 fuse_left chooses for the acc += d*d chains,
+//                                 cross_left for runningDist[0] += runningDist[j]
 //   * value + value            -> plain rounded addition.
 template <typename T>
 struct DevNode {
@@ -144,6 +147,7 @@ bool within(const T* p, const T* c, uint32_t n, T eps, const orc_cfg& cfg) {
     const uint32_t ilp = cfg.ilp;
     const bool fold0 = cfg.sc_contract || cfg.fold_zero;
     const bool left = cfg.fuse_left;
+    const bool xleft = cfg.cross_left;
     auto P = [&](uint32_t l) { return DevNode<T>::make_prod(c[l] - p[l]); };
     if (ilp == 0) {
         // kernel.cu:346-356: runningTotalDist += d*d
@@ -161,13 +165,13 @@ bool within(const T* p, const T* c, uint32_t n, T eps, const orc_cfg& cfg) {
         for (uint32_t j = 0; j < ilp && (l + j) < n; j++) r[j] = dev_add(r[j], P(l + j), fold0, left);
         if (cfg.shortcircuit) {
             for (uint32_t j = 1; j < ilp; j++) {
-                r[0] = dev_add(r[0], r[j], fold0, left);
+                r[0] = dev_add(r[0], r[j], fold0, xleft);
                 r[j] = DevNode<T>::make_zero();
             }
             if (sqrtT<T>(r[0].v) > eps) return false;  // kernel.cu:331-333
         }
     }
-    for (uint32_t j = 1; j < ilp; j++) r[0] = dev_add(r[0], r[j], fold0, left);  // kernel.cu:337-340
+    for (uint32_t j = 1; j < ilp; j++) r[0] = dev_add(r[0], r[j], fold0, xleft);  // kernel.cu:337-340
     return sqrtT<T>(r[0].v) <= eps;
 }
 

@@ -36,6 +36,7 @@ class _Cfg(ctypes.Structure):
         ("nthreads", ctypes.c_uint32),
         ("fold_zero", ctypes.c_uint32),
         ("fuse_left", ctypes.c_uint32),
+        ("cross_left", ctypes.c_uint32),
     ]
 
 
@@ -53,24 +54,27 @@ class OracleConfig:
     nthreads: int = 0
     fold_zero: bool | None = None  # None: the pinned policy of the dtype
     fuse_left: bool | None = None
+    cross_left: bool | None = None
 
     def c(self, dtype=np.float32) -> _Cfg:
-        fz, fl = pinned_policy(dtype, self.ilp)
+        fz, fl, xl = pinned_policy(dtype)
         fz = fz if self.fold_zero is None else self.fold_zero
         fl = fl if self.fuse_left is None else self.fuse_left
+        xl = xl if self.cross_left is None else self.cross_left
         return _Cfg(self.k, int(self.reorder), self.ilp, int(self.shortcircuit), self.model,
-                    int(self.sc_contract), int(self.stamp_ref), self.nthreads, int(fz), int(fl))
+                    int(self.sc_contract), int(self.stamp_ref), self.nthreads, int(fz), int(fl), int(xl))
 
 
-def pinned_policy(dtype, ilp: int = 0) -> tuple[bool, bool]:
-    """(fold_zero, fuse_left) of the reference's device arithmetic, as pinned
-    against the reference's own builds (tests/golden/ref_pins.json): float32
-    keeps fma(d, d, 0); float64 folds it to a pending product and, when both
-    operands of an addition are pending products, fuses the accumulator's
-    in the sequential loop and the added term's in the ILP loop."""
+def pinned_policy(dtype) -> tuple[bool, bool, bool]:
+    """(fold_zero, fuse_left, cross_left) of the reference's device arithmetic,
+    as pinned against the reference's own builds (tests/golden/ref_pins.json):
+    float32 keeps fma(d, d, 0); float64 folds 0 + d*d to a pending product and,
+    when both operands of an addition are pending products, fuses the
+    accumulator's in `acc += d*d` and the added register's in
+    `runningDist[0] += runningDist[j]`."""
     if np.dtype(dtype) == np.float64:
-        return True, ilp == 0
-    return False, False
+        return True, True, False
+    return False, False, False
 
 
 _lib = None

@@ -46,11 +46,11 @@ PIN_CONFIGS = {
     "d18_k6_ilp4_sc": (18, 6, "float32", True, 4, True, False, 30000, 3.0),
     "d90_k6_ilp8_sc": (90, 6, "float32", True, 8, True, True, 8000, 8.0),
     "d5_k3_f64_ilp2_sc": (5, 3, "float64", True, 2, True, True, 30000, 2.0),
-    "d5_k3_f64_plain": (5, 3, "float64", True, 0, False, False, 30000, 2.0),
+    "d5_k3_f64_plain": (5, 3, "float64", True, 0, False, False, 60000, 1.3),
     "d18_k6_f64_ilp8": (18, 6, "float64", True, 8, False, True, 30000, 3.0),
     "d18_k6_f64_ilp8_sc": (18, 6, "float64", True, 8, True, True, 30000, 3.0),
     "d5_k3_f32_ilp8": (5, 3, "float32", True, 8, False, False, 30000, 2.0),
-    "d5_k3_f64_ilp8": (5, 3, "float64", True, 8, False, False, 30000, 2.0),
+    "d5_k3_f64_ilp8": (5, 3, "float64", True, 8, False, False, 60000, 1.3),
     "d3_k3_f64_ilp2": (3, 3, "float64", False, 2, False, False, 30000, 2.0),
     "d5_k3_f32_ilp2_sc": (5, 3, "float32", True, 2, True, True, 30000, 2.0),
 }
@@ -101,8 +101,9 @@ def oracle_variants(O, name, pts):
     out = {}
     for fz in (False, True):
         for fl in (False, True):
-            out[f"fold{int(fz)}_left{int(fl)}"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc,
-                                                                 fold_zero=fz, fuse_left=fl)
+            for xl in (False, True):
+                out[f"fold{int(fz)}_left{int(fl)}_xleft{int(xl)}"] = O.OracleConfig(
+                    k=k, reorder=reorder, ilp=ilp, shortcircuit=sc, fold_zero=fz, fuse_left=fl, cross_left=xl)
     out["pinned"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc)
     out["host_unfused"] = O.OracleConfig(k=k, reorder=reorder, ilp=0, model=O.MODEL_HOST)
     return out
@@ -192,3 +193,20 @@ def main():
 
 if __name__ == "__main__":
     main()
+
+
+def merge_into_golden(*result_files: str) -> None:
+    """Folds reference-run results into tests/golden/ref_pins.json (the
+    committed fixture: input spec, the reference's total and the digest of its
+    sorted per-point lists)."""
+    path = os.path.join(HERE, "ref_pins.json")
+    gold = json.load(open(path)) if os.path.exists(path) else {}
+    keep = ("config", "N", "n", "k", "dtype", "reorder", "ilp", "shortcircuit", "query_reorder", "eps",
+            "reference_total", "reference_lists_sha256")
+    for f in result_files:
+        for name, rec in json.load(open(f)).items():
+            if rec.get("status") == "ok":
+                gold[name] = {k: rec[k] for k in keep}
+                gold[name]["gpu_stats_line"] = ", ".join(rec["gpu_stats_line"].split(", ")[2:])
+    with open(path, "w") as fh:
+        json.dump(gold, fh, indent=1, sort_keys=True)
