@@ -138,7 +138,7 @@ struct gsj_context {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaEvent_t tev[6] = {};  // stage timing: index start/end, count start/end, fill start/end
     // device pool
-    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, hkeys, hvals, order, sizes, nchunks,
+    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, hkeys, hvals, order, sizes, nchunks,
         item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
         minmax_part;
     PinnedBuf stage[2];
@@ -446,15 +446,19 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     S.kernel_launches += 1;
     GSJ_CUDA(c, launch_gather_points<T>(d_in, N, n, npad, d_perm, ids, pts, st));
 
-    // ---- cell lookup: dense table when the grid is small, else a hash table
-    uint32_t* dense = nullptr;
+    // ---- cell lookup: on dense grids a slot-prefix table over every linear
+    // cell id (cell L holds slots [ds[L], ds[L+1])), else a hash table of the
+    // non-empty cells
+    uint32_t *ds = nullptr, *dcnt = nullptr;
     unsigned long long* hkeys = nullptr;
     uint32_t* hvals = nullptr;
     uint64_t hmask = 0;
-    const uint64_t dense_limit = std::max<uint64_t>(1u << 24, 4ull * N);
-    if (totalCells <= dense_limit && totalCells <= (1ull << 30)) {
-        GSJ_TRY(dev_get(c, c->dense, totalCells, &dense));
-        GSJ_CUDA(c, cudaMemsetAsync(dense, 0, totalCells * sizeof(uint32_t), st));
+    const uint64_t dense_limit = std::max<uint64_t>(1u << 24, 8ull * N);
+    const bool dense = totalCells <= dense_limit && totalCells < (1ull << 30);
+    if (dense) {
+        GSJ_TRY(dev_get(c, c->dense, totalCells + 1, &ds));
+        GSJ_TRY(dev_get(c, c->dcnt, totalCells + 1, &dcnt));
+        GSJ_CUDA(c, cudaMemsetAsync(dcnt, 0, (totalCells + 1) * sizeof(uint32_t), st));
     } else {
         uint64_t hcap = 1024;
         while (hcap < 2ull * M) hcap <<= 1;
@@ -464,7 +468,12 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_CUDA(c, cudaMemsetAsync(hkeys, 0xff, hcap * sizeof(unsigned long long), st));
     }
     S.kernel_launches += 2;
-    GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, M, (uint32_t)N, dense, hkeys, hvals, hmask, st));
+    GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, runs, M, (uint32_t)N, dcnt, hkeys, hvals, hmask, st));
+    if (dense) {
+        GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tb, dcnt, ds, (int)(totalCells + 1), st));
+        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+        GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(temp, tb, dcnt, ds, (int)(totalCells + 1), st));
+    }
 
     // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525)
     uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
@@ -521,7 +530,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.ids = ids;
     a.cell_start = cell_start;
     a.cell_key = cell_key;
-    a.dense = dense;
+    a.ds = ds;
     a.hkeys = reinterpret_cast<const uint64_t*>(hkeys);
     a.hvals = hvals;
     a.hmask = hmask;
@@ -533,19 +542,27 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.ilp = cfg.ilp;
     a.g = g;
     a.thr = threshold_of<T>(eps);
+    a.eps = eps;
+    for (uint32_t j = 0; j < k; j++) a.minv[j] = minArr[j];
     a.fwd_cnt = fwd;
     a.rev_cnt = rev;
     a.cand_cnt = cand;
     const int model = model_of(cfg);
     const bool stamp = cfg.stamp != 0;
+    // Dense low-dimensional grids use the row-range traversal.  There the
+    // distance work is cheap, so the fill pass walks the full neighbourhood and
+    // writes every list forward only (contiguous, deterministic); the count
+    // pass keeps the unicomp traversal of STAMP.  The pair set is the same.
+    const bool rows = dense && k <= 3;
+    const bool fill_stamp = stamp && !rows;
     GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_join<T>(a, kCount, model, stamp, c->num_sms, st));
+    GSJ_CUDA(c, launch_join<T>(a, kCount, model, stamp, rows, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
 
     // ---- list lengths and offsets
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_sum_counts(fwd, rev, N, counts, st));
+    GSJ_CUDA(c, launch_sum_counts(fwd, rev, ids, N, counts, st));
     void* stemp = nullptr;
     GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
     S.kernel_launches += 3;
@@ -562,7 +579,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     GSJ_TRY(dev_get(c, c->revcur, N, &revcur));
     GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_rev_cursor(offsets, fwd, N, revcur, st));
+    GSJ_CUDA(c, launch_rev_cursor(offsets, fwd, ids, N, revcur, st));
     GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st));
     a.offsets = offsets;
     a.rev_cursor = revcur;
@@ -571,7 +588,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.err_flag = ctr + 1;  // zeroed with the counters before the count pass
     GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_join<T>(a, kFill, model, stamp, c->num_sms, st));
+    GSJ_CUDA(c, launch_join<T>(a, kFill, model, fill_stamp, rows, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
     GSJ_CUDA(c, cudaStreamSynchronize(st));
     {
@@ -666,7 +683,7 @@ int gsj_destroy(gsj_context* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamSynchronize(c->st2);
     Buf* bufs[] = {&c->in,       &c->pts,   &c->ids,    &c->keys,      &c->keys2,   &c->vals,      &c->cell_key,
-                   &c->runs,     &c->cell_start, &c->dense, &c->hkeys, &c->hvals,   &c->order,     &c->sizes,
+                   &c->runs,     &c->cell_start, &c->dense, &c->dcnt, &c->hkeys, &c->hvals, &c->order, &c->sizes,
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
                    &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
                    &c->minarr,   &c->minmax_part};

@@ -9,7 +9,6 @@ namespace gsj {
 constexpr int kMaxK = 10;        // indexed dimensions supported (3^10 neighbour offsets)
 constexpr int kMaxIlp = 64;      // ILP register blocks supported
 constexpr int kQChunk = 32;      // queries per work item (one per lane)
-constexpr uint32_t kCrossBit = 0x80000000u;  // neighbour entry visited across cells (unicomp)
 constexpr uint64_t kEmptyKey = ~0ull;        // hash table empty slot
 
 // Arithmetic order of the squared-distance sum, i.e. the reference's
@@ -34,7 +33,7 @@ struct JoinArgs {
     const uint32_t* ids;          // [N] slot -> original point id
     const uint32_t* cell_start;   // [M+1]
     const uint64_t* cell_key;     // [M]
-    const uint32_t* dense;        // [totalCells] cell index + 1 (0 = empty), or null
+    const uint32_t* ds;           // [totalCells+1] slot prefix over all linear ids (dense grids), or null
     const uint64_t* hkeys;        // [hcap] hash table keys (kEmptyKey = empty), or null
     const uint32_t* hvals;        // [hcap] cell indices
     uint64_t hmask;               // hcap - 1
@@ -44,13 +43,15 @@ struct JoinArgs {
     uint32_t n, npad, ilp;
     GridGeom g;
     T thr;                        // s <= thr  <=>  sqrt(s) <= eps
+    T eps;                        // epsilon in T (cell formula)
+    T minv[kMaxK];                // minArr (grid origin per indexed dim)
     // count pass
-    uint32_t* fwd_cnt;            // [N] by original id
-    uint32_t* rev_cnt;            // [N] by original id (unicomp reverse hits)
+    uint32_t* fwd_cnt;            // [N] by slot
+    uint32_t* rev_cnt;            // [N] by slot (unicomp reverse hits)
     unsigned long long* cand_cnt; // candidate evaluations
     // fill pass
     const uint64_t* offsets;      // [N+1] by original id
-    unsigned long long* rev_cursor;  // [N] next free reverse slot by original id
+    unsigned long long* rev_cursor;  // [N] next free reverse entry, by slot
     uint32_t* table;              // [R]
     unsigned long long table_cap; // R: writes at or beyond it are dropped and flagged
     uint32_t* err_flag;           // set to 1 when a write would leave the table

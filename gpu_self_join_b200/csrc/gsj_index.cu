@@ -164,9 +164,12 @@ __global__ void k_cell_start_tail(uint32_t* cell_start, uint32_t M, uint32_t N) 
     if (threadIdx.x == 0 && blockIdx.x == 0) cell_start[M] = N;
 }
 
-__global__ void k_dense_fill(const uint64_t* __restrict__ cell_key, uint32_t M, uint32_t* __restrict__ dense) {
+// Points per linear cell id (zero elsewhere); its exclusive scan is the
+// slot-prefix table ds: cell L holds slots [ds[L], ds[L+1]).
+__global__ void k_dense_counts(const uint64_t* __restrict__ cell_key, const uint32_t* __restrict__ sizes, uint32_t M,
+                               uint32_t* __restrict__ dcnt) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < M) dense[cell_key[c]] = c + 1;
+    if (c < M) dcnt[cell_key[c]] = sizes[c];
 }
 
 __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, uint32_t M, unsigned long long* hkeys,
@@ -212,16 +215,18 @@ __global__ void k_iota(uint32_t* __restrict__ out, uint32_t M) {
 }
 
 // Neighbour counts -> list lengths -> cursors.
-__global__ void k_sum_counts(const uint32_t* __restrict__ fwd, const uint32_t* __restrict__ rev, uint64_t N,
-                             uint32_t* __restrict__ total) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i < N) total[i] = fwd[i] + rev[i];
+// List lengths in point-id order from the per-slot counts: total[ids[s]] = fwd[s] + rev[s].
+__global__ void k_sum_counts(const uint32_t* __restrict__ fwd, const uint32_t* __restrict__ rev,
+                             const uint32_t* __restrict__ ids, uint64_t N, uint32_t* __restrict__ total) {
+    const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s < N) total[ids[s]] = fwd[s] + rev[s];
 }
 
-__global__ void k_rev_cursor(const uint64_t* __restrict__ offsets, const uint32_t* __restrict__ fwd, uint64_t N,
-                             unsigned long long* __restrict__ cur) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i < N) cur[i] = offsets[i] + fwd[i];
+// Reverse-entry cursors by slot: the reverse part of a list follows its forward part.
+__global__ void k_rev_cursor(const uint64_t* __restrict__ offsets, const uint32_t* __restrict__ fwd,
+                             const uint32_t* __restrict__ ids, uint64_t N, unsigned long long* __restrict__ cur) {
+    const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s < N) cur[s] = offsets[ids[s]] + fwd[s];
 }
 
 // ------------------------------------------------------------ launchers
@@ -256,11 +261,11 @@ cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t n
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, uint32_t M, uint32_t N,
-                               uint32_t* dense, unsigned long long* hkeys, uint32_t* hvals, uint64_t hmask,
-                               cudaStream_t st) {
+cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, const uint32_t* sizes, uint32_t M,
+                               uint32_t N, uint32_t* dcnt, unsigned long long* hkeys, uint32_t* hvals,
+                               uint64_t hmask, cudaStream_t st) {
     k_cell_start_tail<<<1, 32, 0, st>>>(cell_start, M, N);
-    if (dense) k_dense_fill<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, M, dense);
+    if (dcnt) k_dense_counts<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, sizes, M, dcnt);
     if (hkeys) k_hash_insert<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, M, hkeys, hvals, hmask);
     return cudaGetLastError();
 }
@@ -282,15 +287,15 @@ cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, uint64_t N, uint32_t* total,
-                              cudaStream_t st) {
-    k_sum_counts<<<blocks_for(N, 256), 256, 0, st>>>(fwd, rev, N, total);
+cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, const uint32_t* ids, uint64_t N,
+                              uint32_t* total, cudaStream_t st) {
+    k_sum_counts<<<blocks_for(N, 256), 256, 0, st>>>(fwd, rev, ids, N, total);
     return cudaGetLastError();
 }
 
-cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, uint64_t N, unsigned long long* cur,
-                              cudaStream_t st) {
-    k_rev_cursor<<<blocks_for(N, 256), 256, 0, st>>>(offsets, fwd, N, cur);
+cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, const uint32_t* ids, uint64_t N,
+                              unsigned long long* cur, cudaStream_t st) {
+    k_rev_cursor<<<blocks_for(N, 256), 256, 0, st>>>(offsets, fwd, ids, N, cur);
     return cudaGetLastError();
 }
 

@@ -65,21 +65,33 @@ __host__ __device__ inline WarpSmem warp_smem_layout(uint32_t npad, uint32_t tsi
     return w;
 }
 
+// Slot range of the cell with linear id `lin`: from the dense slot-prefix
+// table (ds[lin] .. ds[lin+1]) or through the hash table of non-empty cells.
 template <typename T>
-__device__ __forceinline__ int lookup_cell(const JoinArgs<T>& a, uint64_t lin) {
-    if (a.dense) return (int)a.dense[lin] - 1;
+__device__ __forceinline__ bool lookup_range(const JoinArgs<T>& a, uint64_t lin, uint32_t& start, uint32_t& cnt) {
+    if (a.ds) {
+        start = a.ds[lin];
+        cnt = a.ds[lin + 1] - start;
+        return cnt != 0;
+    }
     uint64_t h = mix64(lin) & a.hmask;
     for (uint64_t p = 0; p <= a.hmask; p++) {
         const uint64_t kk = a.hkeys[h];
-        if (kk == lin) return (int)a.hvals[h];
-        if (kk == kEmptyKey) return -1;
+        if (kk == lin) {
+            const uint32_t c = a.hvals[h];
+            start = a.cell_start[c];
+            cnt = a.cell_start[c + 1] - start;
+            return true;
+        }
+        if (kk == kEmptyKey) return false;
         h = (h + 1) & a.hmask;
     }
-    return -1;
+    return false;
 }
 
-template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS>
-__global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff) {
+template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS, bool ROWS>
+__global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff,
+                                              uint32_t batch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool GENERIC = (NT == 0);
     const unsigned FULL = 0xffffffffu;
@@ -97,60 +109,111 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
     const uint32_t k = a.g.k;
     unsigned long long cand_total = 0;
 
+    // work items are claimed `batch` at a time (one atomic per batch)
+    uint32_t item = 0, item_end = 0;
     for (;;) {
-        uint32_t item = 0;
-        if (lane == 0) item = atomicAdd(a.work_counter, 1u);
-        item = __shfl_sync(FULL, item, 0);
-        if (item >= a.num_items) break;
-        const uint2 wi = a.items[item];
+        if (item >= item_end) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(a.work_counter, batch);
+            base = __shfl_sync(FULL, base, 0);
+            if (base >= a.num_items) break;
+            item = base;
+            item_end = min(base + batch, a.num_items);
+        }
+        const uint2 wi = a.items[item++];
         const uint32_t cell = wi.x;
         const uint32_t cs = a.cell_start[cell], ce = a.cell_start[cell + 1];
         const uint32_t q0 = cs + wi.y * kQChunk;
         const uint32_t qn = min((uint32_t)kQChunk, ce - q0);
 
-        // ---- own cell coordinates from the linear id
-        uint32_t own[kMaxK];
-        const uint64_t key = a.cell_key[cell];
-#pragma unroll
-        for (int j = 0; j < kMaxK; j++) own[j] = (j < (int)k) ? (uint32_t)((key / a.g.mult[j]) % a.g.ncells[j]) : 0u;
-
-        // ---- neighbour cells (kernel.cu:180-303; stamploops.h for STAMP)
         uint32_t nnb = 0;
-        for (uint32_t base = 0; base < noff; base += 32) {
-            const uint32_t o = base + lane;
-            bool ok = o < noff;
-            uint64_t lin = 0;
-            bool moved = false, hd_odd = false;
-            uint32_t t = o;
-#pragma unroll
-            for (int j = 0; j < kMaxK; j++) {
-                if (j < (int)k) {
-                    const int dl = (int)(t % 3u) - 1;
-                    t /= 3u;
-                    const long long nbj = (long long)own[j] + dl;
-                    if (nbj < 0 || nbj >= (long long)a.g.ncells[j]) ok = false;
-                    lin += (uint64_t)nbj * a.g.mult[j];
-                    if (dl != 0) {
-                        moved = true;
-                        hd_odd = (own[j] & 1u) != 0;  // highest differing dim wins
-                    }
+        if constexpr (ROWS) {
+            // ---- dense grid, k <= 3: the 3 cells x-1..x+1 of a neighbour row are
+            // consecutive linear ids, hence one contiguous slot range
+            // [ds[row + xlo], ds[row + xhi + 1]).  3^(k-1) rows per cell.
+            const uint32_t key = (uint32_t)a.cell_key[cell];
+            const uint32_t n0 = a.g.ncells[0];
+            const uint32_t o0 = key % n0;
+            const uint32_t rest = key / n0;
+            const uint32_t o1 = k >= 2 ? rest % a.g.ncells[1] : 0u;
+            const uint32_t o2 = k >= 3 ? rest / a.g.ncells[1] : 0u;
+            const uint32_t nrows = k == 1 ? 1u : (k == 2 ? 3u : 9u);
+            const int d1 = k >= 2 ? (int)(lane % 3) - 1 : 0;
+            const int d2 = k >= 3 ? (int)(lane / 3) - 1 : 0;
+            bool ok = (uint32_t)lane < nrows;
+            const long long r1 = (long long)o1 + d1, r2 = (long long)o2 + d2;
+            if (k >= 2 && (r1 < 0 || r1 >= (long long)a.g.ncells[1])) ok = false;
+            if (k >= 3 && (r2 < 0 || r2 >= (long long)a.g.ncells[2])) ok = false;
+            uint32_t xlo = o0 > 0 ? o0 - 1u : 0u;
+            uint32_t xhi = o0 + 1u < n0 ? o0 + 1u : n0 - 1u;
+            if (STAMP) {
+                // stamploops.h: own row -> dim-0 neighbours only when x is odd;
+                // another row -> all three cells when the own coordinate of its
+                // highest differing dim is odd
+                if (d1 == 0 && d2 == 0) {
+                    if (!(o0 & 1u)) xlo = xhi = o0;
+                } else {
+                    const bool odd = d2 != 0 ? (o2 & 1u) != 0u : (o1 & 1u) != 0u;
+                    if (!odd) ok = false;
                 }
             }
-            // unicomp: a neighbour whose highest differing dim d has an even own
-            // coordinate is visited from the other cell (stamploops.h: `nDCellIDs[d] & 1`)
-            if (STAMP && moved && !hd_odd) ok = false;
-            const bool cross = STAMP && moved;
-            int c = -1;
-            if (ok) c = lookup_cell(a, lin);
-            const bool found = c >= 0;
+            uint32_t lo = 0, cnt = 0;
+            if (ok) {
+                const uint32_t rowbase = (uint32_t)r1 * n0 + (uint32_t)r2 * (uint32_t)a.g.mult[2 < kMaxK ? 2 : 0];
+                lo = a.ds[rowbase + xlo];
+                cnt = a.ds[rowbase + xhi + 1u] - lo;
+            }
+            const bool found = ok && cnt != 0u;
             const unsigned m = __ballot_sync(FULL, found);
             if (found) {
-                const uint32_t pos = nnb + __popc(m & lt);
-                const uint32_t st = a.cell_start[c];
-                nb_start[pos] = st | (cross ? kCrossBit : 0u);
-                nb_pref[pos] = a.cell_start[c + 1] - st;
+                const uint32_t pos = __popc(m & lt);
+                nb_start[pos] = lo;
+                nb_pref[pos] = cnt;
             }
-            nnb += __popc(m);
+            nnb = __popc(m);
+        } else {
+            // ---- own cell coordinates, from the first query of the cell with the
+            // formula the keys were built with (main.cu:744, kernel.cu:184)
+            uint32_t own[kMaxK];
+#pragma unroll
+            for (int j = 0; j < kMaxK; j++)
+                own[j] = (j < (int)k) ? FP<T>::to_uint_rz(FP<T>::div(FP<T>::sub(a.pts[(size_t)cs * npad + j], a.minv[j]),
+                                                                       a.eps))
+                                      : 0u;
+            // ---- neighbour cells (kernel.cu:180-303; stamploops.h for STAMP)
+            for (uint32_t base = 0; base < noff; base += 32) {
+                const uint32_t o = base + lane;
+                bool ok = o < noff;
+                uint64_t lin = 0;
+                bool moved = false, hd_odd = false;
+                uint32_t t = o;
+#pragma unroll
+                for (int j = 0; j < kMaxK; j++) {
+                    if (j < (int)k) {
+                        const int dl = (int)(t % 3u) - 1;
+                        t /= 3u;
+                        const long long nbj = (long long)own[j] + dl;
+                        if (nbj < 0 || nbj >= (long long)a.g.ncells[j]) ok = false;
+                        lin += (uint64_t)nbj * a.g.mult[j];
+                        if (dl != 0) {
+                            moved = true;
+                            hd_odd = (own[j] & 1u) != 0;  // highest differing dim wins
+                        }
+                    }
+                }
+                // unicomp: a neighbour whose highest differing dim d has an even own
+                // coordinate is visited from the other cell (stamploops.h: `nDCellIDs[d] & 1`)
+                if (STAMP && moved && !hd_odd) ok = false;
+                uint32_t st = 0, cnt = 0;
+                const bool found = ok && lookup_range(a, lin, st, cnt);
+                const unsigned m = __ballot_sync(FULL, found);
+                if (found) {
+                    const uint32_t pos = nnb + __popc(m & lt);
+                    nb_start[pos] = st;
+                    nb_pref[pos] = cnt;
+                }
+                nnb += __popc(m);
+            }
         }
         __syncwarp();
         // exclusive prefix of candidate counts over the list
@@ -188,9 +251,8 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
             bool cross = false;
             if (valid) {
                 while (nb_pref[ent + 1] <= f) ent++;
-                const uint32_t st = nb_start[ent];
-                cross = (st & kCrossBit) != 0u;
-                slot = (st & ~kCrossBit) + (f - nb_pref[ent]);
+                slot = nb_start[ent] + (f - nb_pref[ent]);
+                cross = STAMP && (slot < cs || slot >= ce);  // outside the own cell
                 corig = a.ids[slot];
             }
             T creg[NT > 0 ? NT : 1];
@@ -230,9 +292,9 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                 }
             }
             if (PASS == kCount) {
-                if (STAMP && myrev) atomicAdd(&a.rev_cnt[corig], myrev);
+                if (STAMP && myrev) atomicAdd(&a.rev_cnt[slot], myrev);
             } else if (STAMP && revmask) {
-                unsigned long long pos = atomicAdd(&a.rev_cursor[corig], (unsigned long long)__popc(revmask));
+                unsigned long long pos = atomicAdd(&a.rev_cursor[slot], (unsigned long long)__popc(revmask));
                 while (revmask) {
                     const int j = __ffs(revmask) - 1;
                     revmask &= revmask - 1u;
@@ -243,16 +305,16 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
             }
             __syncwarp();
         }
-        if (PASS == kCount && lane < qn) a.fwd_cnt[qid_s[lane]] = myq;
+        if (PASS == kCount && lane < qn) a.fwd_cnt[q0 + lane] = myq;
         __syncwarp();
     }
     if (PASS == kCount && lane == 0 && cand_total) atomicAdd(a.cand_cnt, cand_total);
 }
 
 // ------------------------------------------------------------------ launch
-template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS>
+template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS, bool ROWS>
 static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, int num_sms, cudaStream_t st) {
-    auto kern = k_join<T, NT, MODEL, POL, STAMP, PASS>;
+    auto kern = k_join<T, NT, MODEL, POL, STAMP, PASS, ROWS>;
     const WarpSmem L = warp_smem_layout(a.npad, sizeof(T), nb_cap, NT == 0);
     const uint32_t max_smem = 200u * 1024u;
     int warps = (int)(max_smem / L.total);
@@ -269,50 +331,66 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     const uint64_t needed = ((uint64_t)a.num_items + warps - 1) / warps;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > needed) blocks = needed ? needed : 1;
-    kern<<<(unsigned)blocks, threads, smem, st>>>(a, nb_cap, noff);
+    const uint64_t total_warps = blocks * (uint64_t)warps;
+    uint64_t batch = a.num_items / (total_warps * 16u);
+    batch = batch < 1 ? 1 : (batch > 32 ? 32 : batch);
+    kern<<<(unsigned)blocks, threads, smem, st>>>(a, nb_cap, noff, (uint32_t)batch);
     return cudaGetLastError();
 }
 
 template <typename T, int MODEL, int POL, bool STAMP, int PASS>
-static cudaError_t dispatch_nt(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, int num_sms, cudaStream_t st) {
+static cudaError_t dispatch_nt(const JoinArgs<T>& a, bool rows, uint32_t nb_cap, uint32_t noff, int num_sms,
+                               cudaStream_t st) {
+    if (rows) {
+        // low-dimensional dense grids (k <= 3): registers for n <= 4
+        if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
+            switch (a.n) {
+                case 1: return launch_one<T, 1, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
+                case 2: return launch_one<T, 2, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
+                case 3: return launch_one<T, 3, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
+                case 4: return launch_one<T, 4, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
+                default: break;
+            }
+        }
+        return launch_one<T, 0, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
+    }
     if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
         switch (a.n) {
-            case 2: return launch_one<T, 2, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 3: return launch_one<T, 3, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 4: return launch_one<T, 4, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 6: return launch_one<T, 6, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-            case 8: return launch_one<T, 8, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+            case 6: return launch_one<T, 6, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, num_sms, st);
+            case 8: return launch_one<T, 8, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, num_sms, st);
             default: break;
         }
     }
-    return launch_one<T, 0, MODEL, POL, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+    return launch_one<T, 0, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, num_sms, st);
 }
 
 template <typename T, bool STAMP, int PASS>
-static cudaError_t dispatch_model(const JoinArgs<T>& a, int model, uint32_t nb_cap, uint32_t noff, int num_sms,
-                                  cudaStream_t st) {
+static cudaError_t dispatch_model(const JoinArgs<T>& a, int model, bool rows, uint32_t nb_cap, uint32_t noff,
+                                  int num_sms, cudaStream_t st) {
     constexpr int P = sizeof(T) == 8 ? kPolF64 : kPolF32;
     switch (model) {
-        case kSeq: return dispatch_nt<T, kSeq, P, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-        case kIlp: return dispatch_nt<T, kIlp, P, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
-        case kIlpSc: return dispatch_nt<T, kIlpSc, P, STAMP, PASS>(a, nb_cap, noff, num_sms, st);
+        case kSeq: return dispatch_nt<T, kSeq, P, STAMP, PASS>(a, rows, nb_cap, noff, num_sms, st);
+        case kIlp: return dispatch_nt<T, kIlp, P, STAMP, PASS>(a, rows, nb_cap, noff, num_sms, st);
+        case kIlpSc: return dispatch_nt<T, kIlpSc, P, STAMP, PASS>(a, rows, nb_cap, noff, num_sms, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <typename T>
-cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, int num_sms, cudaStream_t st) {
+cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, bool rows, int num_sms,
+                        cudaStream_t st) {
     uint32_t noff = 1;
     for (uint32_t j = 0; j < a.g.k; j++) noff *= 3u;
-    const uint32_t nb_cap = noff;
+    if (rows && (a.g.k > 3 || !a.ds)) return cudaErrorInvalidValue;
+    const uint32_t nb_cap = rows ? 32u : noff;
     if (pass == kCount)
-        return stamp ? dispatch_model<T, true, kCount>(a, model, nb_cap, noff, num_sms, st)
-                     : dispatch_model<T, false, kCount>(a, model, nb_cap, noff, num_sms, st);
-    return stamp ? dispatch_model<T, true, kFill>(a, model, nb_cap, noff, num_sms, st)
-                 : dispatch_model<T, false, kFill>(a, model, nb_cap, noff, num_sms, st);
+        return stamp ? dispatch_model<T, true, kCount>(a, model, rows, nb_cap, noff, num_sms, st)
+                     : dispatch_model<T, false, kCount>(a, model, rows, nb_cap, noff, num_sms, st);
+    return stamp ? dispatch_model<T, true, kFill>(a, model, rows, nb_cap, noff, num_sms, st)
+                 : dispatch_model<T, false, kFill>(a, model, rows, nb_cap, noff, num_sms, st);
 }
 
-template cudaError_t launch_join<float>(const JoinArgs<float>&, int, int, bool, int, cudaStream_t);
-template cudaError_t launch_join<double>(const JoinArgs<double>&, int, int, bool, int, cudaStream_t);
+template cudaError_t launch_join<float>(const JoinArgs<float>&, int, int, bool, bool, int, cudaStream_t);
+template cudaError_t launch_join<double>(const JoinArgs<double>&, int, int, bool, bool, int, cudaStream_t);
 
 }  // namespace gsj

@@ -21,22 +21,26 @@ cudaError_t launch_cell_keys(const T* in, uint64_t N, uint32_t n, const uint32_t
 template <typename T>
 cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t npad, const uint32_t* perm,
                                  const uint32_t* ids, T* pts, cudaStream_t st);
-cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, uint32_t M, uint32_t N,
-                               uint32_t* dense, unsigned long long* hkeys, uint32_t* hvals, uint64_t hmask,
-                               cudaStream_t st);
+// cell_start[M] = N; then either the dense per-linear-id point counts
+// (dcnt[key] = size, to be scanned into the slot-prefix table) or the hash table.
+cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, const uint32_t* sizes, uint32_t M,
+                               uint32_t N, uint32_t* dcnt, unsigned long long* hkeys, uint32_t* hvals,
+                               uint64_t hmask, cudaStream_t st);
 cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t* nchunks,
                                uint32_t* sizes, cudaStream_t st);
 cudaError_t launch_make_items(const uint32_t* order, const uint32_t* nchunks, const uint32_t* item_off,
                               uint32_t M, uint2* items, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st);
-cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, uint64_t N, uint32_t* total,
-                              cudaStream_t st);
-cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, uint64_t N, unsigned long long* cur,
-                              cudaStream_t st);
+cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, const uint32_t* ids, uint64_t N,
+                              uint32_t* total, cudaStream_t st);
+cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, const uint32_t* ids, uint64_t N,
+                              unsigned long long* cur, cudaStream_t st);
 
 // Join passes.  `pass` is kCount or kFill; `model` one of Model; `stamp`
 // selects the unicomp traversal.  The launcher picks the specialisation.
+// `rows` selects the dense low-dimensional specialisation (k <= 3, a.ds set).
 template <typename T>
-cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, int num_sms, cudaStream_t st);
+cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, bool rows, int num_sms,
+                        cudaStream_t st);
 
 }  // namespace gsj
