@@ -18,6 +18,7 @@ GSJ_FLOAT32 = 0
 GSJ_FLOAT64 = 1
 GSJ_FLAG_SORT_LISTS = 0x1
 GSJ_FLAG_QUIET = 0x2
+GSJ_FLAG_NO_UNICOMP = 0x4
 
 # Every symbol declared in include/gpuselfjoin.h.
 EXPORTED_SYMBOLS = (

@@ -138,7 +138,9 @@ struct gsj_context {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaEvent_t tev[6] = {};  // stage timing: index start/end, count start/end, fill start/end
     // device pool
-    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, hkeys, hvals, order, sizes, nchunks,
+    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys,
+        hvals, order,
+        sizes, nchunks,
         item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
         minmax_part;
     PinnedBuf stage[2];
@@ -474,6 +476,25 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
         GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(temp, tb, dcnt, ds, (int)(totalCells + 1), st));
     }
+    // Dense low-dimensional grids use the row-range traversal driven by a
+    // per-cell plan of neighbour-row slot ranges.
+    const bool rows = dense && k <= 3;
+    uint2* plan = nullptr;
+    uint8_t* plan_par = nullptr;
+    if (rows) {
+        const uint32_t nrows = k == 1 ? 1u : (k == 2 ? 3u : 9u);
+        GSJ_TRY(dev_get(c, c->plan, (size_t)M * nrows, &plan));
+        GSJ_TRY(dev_get(c, c->plan_par, M, &plan_par));
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_cell_plan(cell_key, M, g, ds, plan, plan_par, st));
+    }
+    uint32_t* slot_cell = nullptr;
+    const bool tpq = rows && cfg.ilp == 0 && n <= 4;
+    if (tpq) {
+        GSJ_TRY(dev_get(c, c->slot_cell, N, &slot_cell));
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_slot_cell(cell_start, M, slot_cell, st));
+    }
 
     // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525)
     uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
@@ -531,6 +552,8 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.cell_start = cell_start;
     a.cell_key = cell_key;
     a.ds = ds;
+    a.plan = plan;
+    a.plan_par = plan_par;
     a.hkeys = reinterpret_cast<const uint64_t*>(hkeys);
     a.hvals = hvals;
     a.hmask = hmask;
@@ -539,6 +562,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.work_counter = ctr;
     a.n = n;
     a.npad = npad;
+    a.n_points = (uint32_t)N;
     a.ilp = cfg.ilp;
     a.g = g;
     a.thr = threshold_of<T>(eps);
@@ -548,16 +572,19 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.rev_cnt = rev;
     a.cand_cnt = cand;
     const int model = model_of(cfg);
-    const bool stamp = cfg.stamp != 0;
-    // Dense low-dimensional grids use the row-range traversal.  There the
-    // distance work is cheap, so the fill pass walks the full neighbourhood and
-    // writes every list forward only (contiguous, deterministic); the count
-    // pass keeps the unicomp traversal of STAMP.  The pair set is the same.
-    const bool rows = dense && k <= 3;
+    const bool stamp = cfg.stamp != 0 && !(cfg.flags & GSJ_FLAG_NO_UNICOMP);
+    // On the row-range path the distance work is cheap, so the fill pass walks
+    // the full neighbourhood and writes every list forward only (contiguous,
+    // deterministic); the count pass keeps the unicomp traversal of STAMP.  The
+    // pair set is the same either way.
     const bool fill_stamp = stamp && !rows;
     GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_join<T>(a, kCount, model, stamp, rows, c->num_sms, st));
+    // Dense low-dimensional grids count with one thread per query (the full
+    // neighbourhood; the cells there are too small for per-cell warp work);
+    // everything else counts with the warp-per-cell kernel.
+    if (tpq) GSJ_CUDA(c, launch_join_tpq<T>(a, kCount, slot_cell, c->num_sms, st));
+    else GSJ_CUDA(c, launch_join<T>(a, kCount, model, stamp, rows, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
 
     // ---- list lengths and offsets
@@ -683,7 +710,8 @@ int gsj_destroy(gsj_context* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamSynchronize(c->st2);
     Buf* bufs[] = {&c->in,       &c->pts,   &c->ids,    &c->keys,      &c->keys2,   &c->vals,      &c->cell_key,
-                   &c->runs,     &c->cell_start, &c->dense, &c->dcnt, &c->hkeys, &c->hvals, &c->order, &c->sizes,
+                   &c->runs,     &c->cell_start, &c->dense, &c->dcnt, &c->plan, &c->plan_par, &c->slot_cell, &c->hkeys, &c->hvals,
+                   &c->order,    &c->sizes,
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
                    &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
                    &c->minarr,   &c->minmax_part};

@@ -34,6 +34,8 @@ struct JoinArgs {
     const uint32_t* cell_start;   // [M+1]
     const uint64_t* cell_key;     // [M]
     const uint32_t* ds;           // [totalCells+1] slot prefix over all linear ids (dense grids), or null
+    const uint2* plan;            // [M][3^(k-1)] (slot start, count) of each neighbour row (dense, k <= 3)
+    const uint8_t* plan_par;      // [M] parities of the own cell coordinates (bit j = dim j)
     const uint64_t* hkeys;        // [hcap] hash table keys (kEmptyKey = empty), or null
     const uint32_t* hvals;        // [hcap] cell indices
     uint64_t hmask;               // hcap - 1
@@ -41,6 +43,7 @@ struct JoinArgs {
     uint32_t num_items;
     uint32_t* work_counter;       // dynamic work distribution
     uint32_t n, npad, ilp;
+    uint32_t n_points;            // N
     GridGeom g;
     T thr;                        // s <= thr  <=>  sqrt(s) <= eps
     T eps;                        // epsilon in T (cell formula)

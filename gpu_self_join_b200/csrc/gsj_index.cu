@@ -188,6 +188,41 @@ __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, uint32_t M,
     }
 }
 
+// Cell plan of dense low-dimensional grids (k <= 3): for every non-empty
+// cell and each of its 3^(k-1) neighbour rows, the slot range of the row's
+// cells x-1..x+1, clipped to the grid (kernel.cu:180-188 clamp the same way).
+// These cells have consecutive linear ids (dim 0 is fastest), so the range is
+// [ds[row + xlo], ds[row + xhi + 1]).  par holds the parity bit of each own
+// coordinate for the unicomp traversal.
+__global__ void k_cell_plan(const uint64_t* __restrict__ cell_key, uint32_t M, GridGeom g,
+                            const uint32_t* __restrict__ ds, uint2* __restrict__ plan, uint8_t* __restrict__ par) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= M) return;
+    const uint32_t k = g.k;
+    const uint32_t key = (uint32_t)cell_key[c];
+    const uint32_t n0 = g.ncells[0];
+    const uint32_t o0 = key % n0, rest = key / n0;
+    const uint32_t o1 = k >= 2 ? rest % g.ncells[1] : 0u;
+    const uint32_t o2 = k >= 3 ? rest / g.ncells[1] : 0u;
+    const uint32_t nrows = k == 1 ? 1u : (k == 2 ? 3u : 9u);
+    const uint32_t xlo = o0 > 0 ? o0 - 1u : 0u;
+    const uint32_t xhi = o0 + 1u < n0 ? o0 + 1u : n0 - 1u;
+    for (uint32_t r = 0; r < nrows; r++) {
+        const long long r1 = (long long)o1 + (k >= 2 ? (long long)(r % 3) - 1 : 0);
+        const long long r2 = (long long)o2 + (k >= 3 ? (long long)(r / 3) - 1 : 0);
+        uint2 e = make_uint2(0u, 0u);
+        const bool ok = (k < 2 || (r1 >= 0 && r1 < (long long)g.ncells[1])) &&
+                        (k < 3 || (r2 >= 0 && r2 < (long long)g.ncells[2]));
+        if (ok) {
+            const uint32_t rowbase = (uint32_t)r1 * n0 + (k >= 3 ? (uint32_t)r2 * (uint32_t)g.mult[2] : 0u);
+            const uint32_t lo = ds[rowbase + xlo];
+            e = make_uint2(lo, ds[rowbase + xhi + 1u] - lo);
+        }
+        plan[(size_t)c * nrows + r] = e;
+    }
+    par[c] = (uint8_t)((o0 & 1u) | ((o1 & 1u) << 1) | ((o2 & 1u) << 2));
+}
+
 // ------------------------------------------------------------ work items
 // A work item is one chunk of up to kQChunk consecutive query slots of one cell.
 __global__ void k_item_counts(const uint32_t* __restrict__ cell_start, const uint32_t* __restrict__ order,
@@ -267,6 +302,12 @@ cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, c
     k_cell_start_tail<<<1, 32, 0, st>>>(cell_start, M, N);
     if (dcnt) k_dense_counts<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, sizes, M, dcnt);
     if (hkeys) k_hash_insert<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, M, hkeys, hvals, hmask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cell_plan(const uint64_t* cell_key, uint32_t M, const GridGeom& g, const uint32_t* ds,
+                             uint2* plan, uint8_t* par, cudaStream_t st) {
+    k_cell_plan<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, M, g, ds, plan, par);
     return cudaGetLastError();
 }
 

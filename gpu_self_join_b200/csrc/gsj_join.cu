@@ -128,47 +128,31 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
 
         uint32_t nnb = 0;
         if constexpr (ROWS) {
-            // ---- dense grid, k <= 3: the 3 cells x-1..x+1 of a neighbour row are
-            // consecutive linear ids, hence one contiguous slot range
-            // [ds[row + xlo], ds[row + xhi + 1]).  3^(k-1) rows per cell.
-            const uint32_t key = (uint32_t)a.cell_key[cell];
-            const uint32_t n0 = a.g.ncells[0];
-            const uint32_t o0 = key % n0;
-            const uint32_t rest = key / n0;
-            const uint32_t o1 = k >= 2 ? rest % a.g.ncells[1] : 0u;
-            const uint32_t o2 = k >= 3 ? rest / a.g.ncells[1] : 0u;
+            // ---- dense grid, k <= 3: the cell plan holds, per neighbour row, the
+            // slot range of cells x-1..x+1 (one contiguous range, see
+            // k_cell_plan) and the parities of the own coordinates.
             const uint32_t nrows = k == 1 ? 1u : (k == 2 ? 3u : 9u);
-            const int d1 = k >= 2 ? (int)(lane % 3) - 1 : 0;
-            const int d2 = k >= 3 ? (int)(lane / 3) - 1 : 0;
-            bool ok = (uint32_t)lane < nrows;
-            const long long r1 = (long long)o1 + d1, r2 = (long long)o2 + d2;
-            if (k >= 2 && (r1 < 0 || r1 >= (long long)a.g.ncells[1])) ok = false;
-            if (k >= 3 && (r2 < 0 || r2 >= (long long)a.g.ncells[2])) ok = false;
-            uint32_t xlo = o0 > 0 ? o0 - 1u : 0u;
-            uint32_t xhi = o0 + 1u < n0 ? o0 + 1u : n0 - 1u;
+            uint2 e = make_uint2(0u, 0u);
+            if ((uint32_t)lane < nrows) e = a.plan[(size_t)cell * nrows + lane];
             if (STAMP) {
-                // stamploops.h: own row -> dim-0 neighbours only when x is odd;
+                // stamploops.h: own row -> its dim-0 neighbours only when x is odd;
                 // another row -> all three cells when the own coordinate of its
                 // highest differing dim is odd
+                const uint32_t par = a.plan_par[cell];
+                const int d1 = k >= 2 ? (int)(lane % 3) - 1 : 0;
+                const int d2 = k >= 3 ? (int)(lane / 3) - 1 : 0;
                 if (d1 == 0 && d2 == 0) {
-                    if (!(o0 & 1u)) xlo = xhi = o0;
-                } else {
-                    const bool odd = d2 != 0 ? (o2 & 1u) != 0u : (o1 & 1u) != 0u;
-                    if (!odd) ok = false;
+                    if (!(par & 1u)) e = make_uint2(cs, ce - cs);
+                } else if (!((par >> (d2 != 0 ? 2 : 1)) & 1u)) {
+                    e.y = 0u;
                 }
             }
-            uint32_t lo = 0, cnt = 0;
-            if (ok) {
-                const uint32_t rowbase = (uint32_t)r1 * n0 + (uint32_t)r2 * (uint32_t)a.g.mult[2 < kMaxK ? 2 : 0];
-                lo = a.ds[rowbase + xlo];
-                cnt = a.ds[rowbase + xhi + 1u] - lo;
-            }
-            const bool found = ok && cnt != 0u;
+            const bool found = (uint32_t)lane < nrows && e.y != 0u;
             const unsigned m = __ballot_sync(FULL, found);
             if (found) {
                 const uint32_t pos = __popc(m & lt);
-                nb_start[pos] = lo;
-                nb_pref[pos] = cnt;
+                nb_start[pos] = e.x;
+                nb_pref[pos] = e.y;
             }
             nnb = __popc(m);
         } else {
@@ -238,72 +222,151 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
         if (lane < qn) qid_s[lane] = a.ids[q0 + lane];
         __syncwarp();
         if (PASS == kCount) cand_total += (unsigned long long)total * qn;
-        uint32_t myq = 0;
-        unsigned long long mycur = 0;
+        uint32_t myq = 0;                 // count pass: lane j holds query j's forward count
+        unsigned long long mycur = 0;     // fill pass: lane j holds query j's next table position
         if (PASS == kFill && lane < qn) mycur = a.offsets[qid_s[lane]];
 
-        // ---- candidate tiles
-        uint32_t ent = 0;
-        for (uint32_t t0 = 0; t0 < total; t0 += 32) {
-            const uint32_t f = t0 + lane;
-            const bool valid = f < total;
-            uint32_t slot = 0, corig = 0;
-            bool cross = false;
-            if (valid) {
-                while (nb_pref[ent + 1] <= f) ent++;
-                slot = nb_start[ent] + (f - nb_pref[ent]);
-                cross = STAMP && (slot < cs || slot >= ce);  // outside the own cell
-                corig = a.ids[slot];
-            }
-            T creg[NT > 0 ? NT : 1];
-            if (!GENERIC) {
-                const T* row = a.pts + (size_t)slot * npad;
+        if constexpr (!GENERIC) {
+            // ---- register path (n <= 8): up to G tiles of 32 candidates live in
+            // registers; queries outside, tiles inside, so each query's
+            // cursor and coordinates are loaded once per group of tiles.
+            constexpr int G = 4;
+            constexpr int NR = NT > 0 ? NT : 1;
+            uint32_t ent = 0;
+            for (uint32_t g0 = 0; g0 < total; g0 += 32u * G) {
+                T cx[G][NR];
+                uint32_t cid[G], cslot[G];
+                bool cval[G], ccross[G];
+                const uint32_t ntile = min((uint32_t)G, (total - g0 + 31u) / 32u);
 #pragma unroll
-                for (int l = 0; l < (NT > 0 ? NT : 1); l++) creg[l] = row[l];
-            } else {
-                const T* row = a.pts + (size_t)slot * npad;
-                T* dst = cand_s + (size_t)lane * (npad + 1u);
-                for (uint32_t l = 0; l < a.n; l++) dst[l] = row[l];
+                for (int t = 0; t < G; t++) {
+                    const uint32_t f = g0 + (uint32_t)t * 32u + lane;
+                    cval[t] = f < total;
+                    cslot[t] = 0u;
+                    cid[t] = 0u;
+                    ccross[t] = false;
+                    if ((uint32_t)t >= ntile) continue;
+                    uint32_t slot = 0;
+                    if (cval[t]) {
+                        while (nb_pref[ent + 1] <= f) ent++;
+                        slot = nb_start[ent] + (f - nb_pref[ent]);
+                    }
+                    cslot[t] = slot;
+                    ccross[t] = STAMP && cval[t] && (slot < cs || slot >= ce);
+                    cid[t] = (PASS == kFill && cval[t]) ? a.ids[slot] : 0u;
+                    const T* row = a.pts + (size_t)slot * npad;
+#pragma unroll
+                    for (int l = 0; l < NR; l++) cx[t][l] = row[l];
+                }
+                uint32_t rev[G], revmask[G];
+#pragma unroll
+                for (int t = 0; t < G; t++) rev[t] = revmask[t] = 0u;
+                for (uint32_t j = 0; j < qn; j++) {
+                    T q[NR];
+#pragma unroll
+                    for (int l = 0; l < NR; l++) q[l] = q_s[(size_t)j * npad + l];
+                    uint32_t cntj = 0;
+                    unsigned long long cur = 0;
+                    if (PASS == kFill) cur = __shfl_sync(FULL, mycur, j);
+#pragma unroll
+                    for (int t = 0; t < G; t++) {
+                        if ((uint32_t)t < ntile) {
+                            const T s = sqdist_seq_reg<T, NR, POL>(q, cx[t]);
+                            const bool hit = cval[t] && (s <= a.thr);
+                            const unsigned b = __ballot_sync(FULL, hit);
+                            if (PASS == kCount) {
+                                cntj += __popc(b);
+                                if (STAMP && ccross[t] && hit) rev[t]++;
+                            } else {
+                                if (hit) {
+                                    const unsigned long long pos = cur + __popc(b & lt);
+                                    if (pos < a.table_cap) a.table[pos] = cid[t];
+                                    else *a.err_flag = 1u;
+                                }
+                                cur += __popc(b);
+                                if (STAMP && ccross[t] && hit) revmask[t] |= 1u << j;
+                            }
+                        }
+                    }
+                    if (PASS == kCount) {
+                        if (lane == (int)j) myq += cntj;
+                    } else {
+                        if (lane == (int)j) mycur = cur;
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < G; t++) {
+                    if (PASS == kCount) {
+                        if (STAMP && rev[t]) atomicAdd(&a.rev_cnt[cslot[t]], rev[t]);
+                    } else if (STAMP && revmask[t]) {
+                        unsigned long long pos =
+                            atomicAdd(&a.rev_cursor[cslot[t]], (unsigned long long)__popc(revmask[t]));
+                        uint32_t m = revmask[t];
+                        while (m) {
+                            const int j = __ffs(m) - 1;
+                            m &= m - 1u;
+                            if (pos < a.table_cap) a.table[pos] = qid_s[j];
+                            else *a.err_flag = 1u;
+                            pos++;
+                        }
+                    }
+                }
+            }
+        } else {
+            // ---- generic n: one tile of 32 candidate rows staged in shared memory
+            uint32_t ent = 0;
+            for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+                const uint32_t f = t0 + lane;
+                const bool valid = f < total;
+                uint32_t slot = 0, corig = 0;
+                bool cross = false;
+                if (valid) {
+                    while (nb_pref[ent + 1] <= f) ent++;
+                    slot = nb_start[ent] + (f - nb_pref[ent]);
+                    cross = STAMP && (slot < cs || slot >= ce);  // outside the own cell
+                    corig = a.ids[slot];
+                }
+                {
+                    const T* row = a.pts + (size_t)slot * npad;
+                    T* dst = cand_s + (size_t)lane * (npad + 1u);
+                    for (uint32_t l = 0; l < a.n; l++) dst[l] = row[l];
+                    __syncwarp();
+                }
+                uint32_t myrev = 0, revmask = 0;
+                for (uint32_t j = 0; j < qn; j++) {
+                    const T* q = q_s + (size_t)j * npad;
+                    const T s =
+                        sqdist_generic<T, MODEL, POL>(q, cand_s + (size_t)lane * (npad + 1u), a.n, a.ilp, a.thr, valid);
+                    const bool hit = valid && (s <= a.thr);
+                    const unsigned b = __ballot_sync(FULL, hit);
+                    if (PASS == kCount) {
+                        if (lane == (int)j) myq += __popc(b);
+                        if (STAMP && cross && hit) myrev++;
+                    } else {
+                        const unsigned long long cur = __shfl_sync(FULL, mycur, j);
+                        if (hit) {
+                            const unsigned long long pos = cur + __popc(b & lt);
+                            if (pos < a.table_cap) a.table[pos] = corig;
+                            else *a.err_flag = 1u;
+                        }
+                        if (lane == (int)j) mycur += __popc(b);
+                        if (STAMP && cross && hit) revmask |= 1u << j;
+                    }
+                }
+                if (PASS == kCount) {
+                    if (STAMP && myrev) atomicAdd(&a.rev_cnt[slot], myrev);
+                } else if (STAMP && revmask) {
+                    unsigned long long pos = atomicAdd(&a.rev_cursor[slot], (unsigned long long)__popc(revmask));
+                    while (revmask) {
+                        const int j = __ffs(revmask) - 1;
+                        revmask &= revmask - 1u;
+                        if (pos < a.table_cap) a.table[pos] = qid_s[j];
+                        else *a.err_flag = 1u;
+                        pos++;
+                    }
+                }
                 __syncwarp();
             }
-            uint32_t myrev = 0, revmask = 0;
-            for (uint32_t j = 0; j < qn; j++) {
-                const T* q = q_s + (size_t)j * npad;
-                T s;
-                if (!GENERIC) {
-                    if constexpr (NT > 0) s = sqdist_seq_reg<T, NT, POL>(q, creg);
-                } else {
-                    s = sqdist_generic<T, MODEL, POL>(q, cand_s + (size_t)lane * (npad + 1u), a.n, a.ilp, a.thr, valid);
-                }
-                const bool hit = valid && (s <= a.thr);
-                const unsigned b = __ballot_sync(FULL, hit);
-                if (PASS == kCount) {
-                    if (lane == (int)j) myq += __popc(b);
-                    if (STAMP && cross && hit) myrev++;
-                } else {
-                    const unsigned long long cur = __shfl_sync(FULL, mycur, j);
-                    if (hit) {
-                        const unsigned long long pos = cur + __popc(b & lt);
-                        if (pos < a.table_cap) a.table[pos] = corig;
-                        else *a.err_flag = 1u;
-                    }
-                    if (lane == (int)j) mycur += __popc(b);
-                    if (STAMP && cross && hit) revmask |= 1u << j;
-                }
-            }
-            if (PASS == kCount) {
-                if (STAMP && myrev) atomicAdd(&a.rev_cnt[slot], myrev);
-            } else if (STAMP && revmask) {
-                unsigned long long pos = atomicAdd(&a.rev_cursor[slot], (unsigned long long)__popc(revmask));
-                while (revmask) {
-                    const int j = __ffs(revmask) - 1;
-                    revmask &= revmask - 1u;
-                    if (pos < a.table_cap) a.table[pos] = qid_s[j];
-                    else *a.err_flag = 1u;
-                    pos++;
-                }
-            }
-            __syncwarp();
         }
         if (PASS == kCount && lane < qn) a.fwd_cnt[q0 + lane] = myq;
         __syncwarp();

@@ -26,6 +26,8 @@ cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t n
 cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, const uint32_t* sizes, uint32_t M,
                                uint32_t N, uint32_t* dcnt, unsigned long long* hkeys, uint32_t* hvals,
                                uint64_t hmask, cudaStream_t st);
+cudaError_t launch_cell_plan(const uint64_t* cell_key, uint32_t M, const GridGeom& g, const uint32_t* ds,
+                             uint2* plan, uint8_t* par, cudaStream_t st);
 cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t* nchunks,
                                uint32_t* sizes, cudaStream_t st);
 cudaError_t launch_make_items(const uint32_t* order, const uint32_t* nchunks, const uint32_t* item_off,
@@ -42,5 +44,13 @@ cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, cons
 template <typename T>
 cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, bool rows, int num_sms,
                         cudaStream_t st);
+
+// Thread-per-query passes of dense low-dimensional grids (full neighbourhood).
+cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, uint32_t* slot_cell, cudaStream_t st);
+template <typename T>
+bool tpq_supported(const JoinArgs<T>& a);
+template <typename T>
+cudaError_t launch_join_tpq(const JoinArgs<T>& a, int pass, const uint32_t* slot_cell, int num_sms,
+                            cudaStream_t st);
 
 }  // namespace gsj

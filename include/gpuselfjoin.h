@@ -47,6 +47,8 @@ extern "C" {
 /* flags */
 #define GSJ_FLAG_SORT_LISTS 0x1u  /* sort every neighbour list ascending       */
 #define GSJ_FLAG_QUIET      0x2u  /* no progress output on stdout              */
+#define GSJ_FLAG_NO_UNICOMP 0x4u  /* full neighbourhood traversal even with STAMP
+                                     (same pair set, different work split)   */
 
 /*
  * Run-time configuration.  Field names follow params.h of the reference
