@@ -640,6 +640,11 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
 
 }  // namespace
 
+namespace gsj {
+// Error reporting for entry points defined in other translation units.
+int report_error(int code, const std::string& msg) { return fail(nullptr, code, msg); }
+}  // namespace gsj
+
 // ====================================================================== C ABI
 extern "C" {
 

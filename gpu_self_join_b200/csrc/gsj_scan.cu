@@ -10,6 +10,10 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <string>
+
+#include "../../include/gpuselfjoin.h"
 #include "gsj_scan.h"
 
 namespace gsj {
@@ -114,4 +118,56 @@ cudaError_t scan_u32_u64(const uint32_t* in, uint64_t* out, uint64_t n, void* te
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- no allocation
+// Scratch of gsj_list_offsets_noalloc: the per-tile sums of the scan live in
+// a fixed array in the library's device image instead of memory obtained
+// from cudaMalloc.  64 KiB hold the sums of 8191 tiles (plus the total), so
+// one call covers up to 8191 * 4096 = 33,550,336 counts.  Every device that
+// loads the library keeps this array until the process exits.
+constexpr size_t kNoAllocScratchBytes = 64u * 1024u;
+constexpr uint64_t kNoAllocMaxTiles = kNoAllocScratchBytes / sizeof(unsigned long long) - 1u;
+constexpr uint64_t kNoAllocMaxCounts = kNoAllocMaxTiles * kScanTile;
+static __device__ __align__(256) unsigned long long g_noalloc_tile_sums[kNoAllocScratchBytes / sizeof(unsigned long long)];
+
+int report_error(int code, const std::string& msg);
+
 }  // namespace gsj
+
+namespace {
+// Device address of g_noalloc_tile_sums, looked up once per device.  On the
+// host the symbol name only stands for the device array; a kernel must be
+// given the address that cudaGetSymbolAddress returns for the current device.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int gsj_list_offsets_noalloc(const uint32_t* d_counts, uint64_t n, uint64_t* d_offsets, void* stream) {
+    using namespace gsj;
+    if (!d_offsets || (n && !d_counts)) return report_error(GSJ_ERR_INVALID, "null device pointer");
+    if (n > kNoAllocMaxCounts)
+        return report_error(GSJ_ERR_INVALID, "gsj_list_offsets_noalloc: " + std::to_string(n) +
+                                                 " counts exceed the fixed scratch limit of " +
+                                                 std::to_string(kNoAllocMaxCounts));
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return report_error(GSJ_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            e = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_noalloc_tile_sums);
+            if (e != cudaSuccess) {
+                g_noalloc_addr[dev] = nullptr;
+                return report_error(GSJ_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            }
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    // Every tile sum the scan reads is written earlier in the same call, so the
+    // previous call's contents need no clearing.
+    e = scan_u32_u64(d_counts, d_offsets, n, scratch, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return report_error(GSJ_ERR_CUDA, std::string("list offsets scan: ") + cudaGetErrorString(e));
+    return GSJ_OK;
+}

@@ -140,6 +140,31 @@ GSJ_API const char* gsj_last_error(gsj_context* ctx);
 GSJ_API float gsj_threshold_f32(float eps);
 GSJ_API double gsj_threshold_f64(double eps);
 
+/*
+ * List offsets without allocating: d_offsets[i] = d_counts[0] + ... +
+ * d_counts[i-1] for i in [0, n], so d_offsets[n] is the total (the layout of
+ * neighborTable for the numNeighbors in d_counts).  No counterpart in the
+ * reference; it is the scan the join itself uses to lay out its table, made
+ * callable by code that must not allocate device memory: a host framework
+ * whose allocator already reserves (nearly) all device memory for its own
+ * pool, where a cudaMalloc fails or forces the pool to give memory back, and
+ * code on a latency-critical path, where cudaMalloc and cudaFree would
+ * synchronise the device.  The call uses no cudaMalloc, cudaFree or
+ * allocating library routine: its scratch (64 KiB of per-tile sums) is a
+ * fixed array inside the library that every device loading the library keeps
+ * until the process exits.  Limits: n <= 33,550,336; larger n returns
+ * GSJ_ERR_INVALID.  d_counts and d_offsets (n + 1 entries) are device memory of
+ * the calling thread's current device; the work is queued on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) and the call returns
+ * without waiting for it.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and caches it; make that first call
+ * before any stream capture.  All calls share the one array, which keeps the
+ * last call's contents (nothing in it needs to start at zero): calls that
+ * overlap on the GPU, e.g. on two streams at once, race and must be ordered by
+ * the caller.
+ */
+GSJ_API int gsj_list_offsets_noalloc(const uint32_t* d_counts, uint64_t n, uint64_t* d_offsets, void* stream);
+
 /* ---------------------------------------------------------------- drop-in
  * The reference's shared-library ABI (built with -DPYTHON, Makefile:58-77).
  *
