@@ -33,8 +33,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
-import time
 
 import numpy as np
 
@@ -129,21 +127,54 @@ def _traffic_from_profile(kernel: str, workload: str):
     return None
 
 
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "rtree_harness")
+
+
+def _rtree_runs(pts: np.ndarray, w, steps: int, sample: int, threads: int, seed: int = 1) -> dict:
+    """Runs the reference's R-tree self-join code (oracle/_ref/rtree_harness,
+    built from the reference's sources) once: tree over all points, then
+    `steps` rounds of `sample` seeded queries."""
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as td:
+        f = os.path.join(td, "pts.bin")
+        np.ascontiguousarray(pts, dtype=np.float32).tofile(f)
+        out = subprocess.run([HARNESS, f, str(pts.shape[0]), str(pts.shape[1]), repr(float(w.eps)), str(threads),
+                              str(steps), str(sample), str(seed)], capture_output=True, text=True, check=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def _rtree_step_values(r: dict) -> list[float]:
+    N, smp, tb = r["N"], r["sample"], r["build_s"]
+    return [(st["pairs"] * N / smp) / (tb + st["query_s"] * N / smp) for st in r["steps"]]
+
+
+def _rtree_sample_text(r: dict, nsteps: int) -> str:
+    return (f"reference R-tree (RTree.h + tree_index.cpp:191-233, built from the reference's sources): tree over all "
+            f"{r['N']} points built once in {r['build_s']:.2f} s on 1 thread as the reference does; {nsteps} rounds of "
+            f"{r['sample']} seeded queries on {r['threads']} threads; pairs/s extrapolated to the full join "
+            f"(build + all {r['N']} queries)")
+
+
 def _cpu_baseline(pts: np.ndarray, w, budget_s: float = 15.0) -> dict:
-    """The oracle's grid join (a CPU port of algorithm 3) on a bounded query
-    sample of the same workload, all host threads: index over all N points,
-    then the sampled queries; pairs/s is extrapolated to the full join."""
+    """The reference's own CPU self-join (its R-tree search and filter) on a
+    bounded query sample of the same workload, all host threads; the oracle's
+    grid join (a CPU port of algorithm 3) where the harness is not built."""
+    cores = os.cpu_count() or 1
+    N = pts.shape[0]
+    if os.path.exists(HARNESS) and pts.shape[1] == 2:
+        r = _rtree_runs(pts, w, steps=3, sample=min(N, 200_000), threads=cores)
+        v = _rtree_step_values(r)
+        return {"value": statistics.mean(v), "unit": "pairs/s", "cores": cores, "kind": "reference",
+                "sample": _rtree_sample_text(r, 3)}
     from oracle import pyoracle as O
 
     O.lib()
-    N = pts.shape[0]
-    cores = os.cpu_count() or 1
     rng = np.random.default_rng(12345)
     cfg = O.OracleConfig(k=w.k, reorder=w.reorder, ilp=w.ilp, shortcircuit=w.shortcircuit, nthreads=cores)
-    nq = 20000
+    nq = min(N, 20000)
     q = np.sort(rng.choice(N, size=nq, replace=False)).astype(np.uint32)
     tot, si, sq = O.join_sample(pts, w.eps, cfg, q)
-    # grow the sample to fill the budget
     per_q = sq / nq
     nq2 = int(min(N, max(nq, (budget_s - si) / max(per_q, 1e-9))))
     if nq2 > nq * 2:
@@ -153,8 +184,8 @@ def _cpu_baseline(pts: np.ndarray, w, budget_s: float = 15.0) -> dict:
     est_R = tot * (N / nq)
     est_t = si + sq * (N / nq)
     return {"value": est_R / est_t, "unit": "pairs/s", "cores": cores, "kind": "port",
-            "sample": f"grid index over all {N} points ({si:.2f} s) + {nq} seeded queries ({sq:.2f} s); "
-                      f"pairs/s extrapolated to all {N} queries"}
+            "sample": f"oracle grid join: index over all {N} points ({si:.2f} s) + {nq} seeded queries "
+                      f"({sq:.2f} s); pairs/s extrapolated to all {N} queries"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -286,53 +317,41 @@ def _ours(args) -> None:
 
 # ------------------------------------------------------------------ reference arm
 def _reference_arm(args) -> None:
-    """The reference's CPU implementation of the self-join on a bounded sample
-    of the same workload, with all host threads.  Uses the reference's R-tree
-    search + filter (tree_index.cpp:191-233, RTree.h) built from its sources
-    into oracle/_ref/rtree_harness when present, else the oracle port."""
+    """The reference's CPU implementation of the self-join (its R-tree search
+    and filter, tree_index.cpp:191-233, built from its sources into
+    oracle/_ref/rtree_harness) on the same workload with all host threads:
+    the tree is built once over all points, then W + K rounds of seeded
+    queries; each round's value is the pairs/s of the full join extrapolated
+    from it.  Without the harness, the oracle port of algorithm 3 is timed."""
     rank, _, world = _env_rank()
     if rank != 0:
         return
     from gpu_self_join_b200 import synth
 
     w = synth.WORKLOADS[args.workload]
-    pts = synth.generate(args.workload)
+    pts = synth.generate(args.workload, args.points)
     N, n = pts.shape
-    harness = os.path.join(ROOT, "oracle", "_ref", "rtree_harness")
-    vals = []
-    desc = None
-    kind = "port"
     cores = os.cpu_count() or 1
-    for step in range(args.warmup + args.steps):
-        if os.path.exists(harness):
-            kind = "reference"
-            r = _run_rtree_harness(harness, pts, w, cores, seed=step)
-            v, desc = r["value"], r["sample"]
-        else:
-            r = _cpu_baseline(pts, w, budget_s=10.0)
-            v, desc = r["value"], r["sample"]
-        if step >= args.warmup:
-            vals.append(v)
+    if os.path.exists(HARNESS) and n == 2:
+        r = _rtree_runs(pts, w, steps=args.warmup + args.steps, sample=min(N, 200_000), threads=cores)
+        vals = _rtree_step_values(r)[args.warmup:]
+        kind, desc = "reference", _rtree_sample_text(r, args.steps)
+    else:
+        vals = []
+        for _ in range(args.warmup + args.steps):
+            vals.append(_cpu_baseline(pts, w, budget_s=5.0)["value"])
+        vals = vals[args.warmup:]
+        kind, desc = "port", "oracle grid join (CPU port of algorithm 3) on seeded query samples"
     value = statistics.mean(vals)
-    line = {"impl": "reference", "metric": "self-join result pairs/s (2-D, 20M points, STAMP=1)"
-            if args.workload == "c2_gmm2d" else f"self-join result pairs/s ({args.workload})",
-            "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)", "config": {"workload": args.workload, "points": N, "dim": n, "eps": w.eps},
+    metric = ("self-join result pairs/s (2-D, 20M points, STAMP=1)" if args.workload == "c2_gmm2d"
+              else f"self-join result pairs/s ({args.workload})")
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "points": N, "dim": n, "eps": w.eps},
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": kind, "sample": desc},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def _run_rtree_harness(harness, pts, w, cores, seed):
-    import tempfile
-
-    with tempfile.TemporaryDirectory() as td:
-        f = os.path.join(td, "pts.bin")
-        pts.tofile(f)
-        out = subprocess.run([harness, f, str(pts.shape[0]), str(pts.shape[1]), repr(float(w.eps)), str(cores),
-                              "8.0", str(seed)], capture_output=True, text=True, check=True)
-    return json.loads(out.stdout.strip().splitlines()[-1])
 
 
 def main():

@@ -94,3 +94,22 @@ build_one() {
 export -f build_one write_params
 export REF OUT
 printf '%s\n' "${CONFIGS[@]}" | xargs -P "$JOBS" -I{} bash -c 'build_one "$@"' _ {}
+
+# The reference's CPU self-join (R-tree search + filter, tree_index.cpp and
+# RTree.h) behind a timing harness (oracle/ref_rtree_harness.cpp), 2-D float:
+# the reference arm of bench.py.  Plain g++ on the reference's own files.
+build_harness() {
+  local dst="$OUT/rtree_harness"
+  if [ -x "$dst" ]; then echo "have rtree_harness"; return 0; fi
+  local tmp
+  tmp=$(mktemp -d)
+  cp "$REF"/tree_index.cpp "$REF"/tree_index.h "$REF"/RTree.h "$tmp"/
+  cp "$HERE/ref_rtree_harness.cpp" "$tmp"/
+  write_params "$tmp" 2 2 float 0 0 0 0 0 0
+  ( cd "$tmp" && g++ -O3 -std=c++14 -fopenmp tree_index.cpp ref_rtree_harness.cpp -o rtree_harness ) \
+    > "$tmp/build.log" 2>&1 || { echo "harness build failed"; tail -20 "$tmp/build.log"; rm -rf "$tmp"; return 1; }
+  cp "$tmp/rtree_harness" "$dst"
+  rm -rf "$tmp"
+  echo "built rtree_harness"
+}
+build_harness
