@@ -138,8 +138,7 @@ struct gsj_context {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaEvent_t tev[6] = {};  // stage timing: index start/end, count start/end, fill start/end
     // device pool
-    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys,
-        hvals, order,
+    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
         item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
         minmax_part;
@@ -583,7 +582,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     // Dense low-dimensional grids count with one thread per query (the full
     // neighbourhood; the cells there are too small for per-cell warp work);
     // everything else counts with the warp-per-cell kernel.
-    if (tpq) GSJ_CUDA(c, launch_join_tpq<T>(a, kCount, slot_cell, c->num_sms, st));
+    if (tpq) GSJ_CUDA(c, launch_count_tpq<T>(a, slot_cell, c->num_sms, st));
     else GSJ_CUDA(c, launch_join<T>(a, kCount, model, stamp, rows, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
 
@@ -605,8 +604,10 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     uint32_t* table = nullptr;
     GSJ_TRY(dev_get(c, c->revcur, N, &revcur));
     GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
-    S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_rev_cursor(offsets, fwd, ids, N, revcur, st));
+    if (fill_stamp) {
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_rev_cursor(offsets, fwd, ids, N, revcur, st));
+    }
     GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st));
     a.offsets = offsets;
     a.rev_cursor = revcur;
@@ -615,7 +616,10 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.err_flag = ctr + 1;  // zeroed with the counters before the count pass
     GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_join<T>(a, kFill, model, fill_stamp, rows, c->num_sms, st));
+    // Dense low-dimensional grids fill with a warp per 32 consecutive query
+    // slots (consecutive queries share their cell's candidate tiles).
+    if (tpq) GSJ_CUDA(c, launch_fill_q32<T>(a, slot_cell, c->num_sms, st));
+    else GSJ_CUDA(c, launch_join<T>(a, kFill, model, fill_stamp, rows, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
     GSJ_CUDA(c, cudaStreamSynchronize(st));
     {
@@ -715,7 +719,8 @@ int gsj_destroy(gsj_context* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamSynchronize(c->st2);
     Buf* bufs[] = {&c->in,       &c->pts,   &c->ids,    &c->keys,      &c->keys2,   &c->vals,      &c->cell_key,
-                   &c->runs,     &c->cell_start, &c->dense, &c->dcnt, &c->plan, &c->plan_par, &c->slot_cell, &c->hkeys, &c->hvals,
+                   &c->runs,     &c->cell_start, &c->dense, &c->dcnt, &c->plan, &c->plan_par, &c->slot_cell, &c->hkeys,
+                   &c->hvals,
                    &c->order,    &c->sizes,
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
                    &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,

@@ -50,7 +50,9 @@ cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, uint32_t* s
 template <typename T>
 bool tpq_supported(const JoinArgs<T>& a);
 template <typename T>
-cudaError_t launch_join_tpq(const JoinArgs<T>& a, int pass, const uint32_t* slot_cell, int num_sms,
-                            cudaStream_t st);
+cudaError_t launch_count_tpq(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st);
+// Fill pass of dense low-dimensional grids: a warp per 32 consecutive query slots.
+template <typename T>
+cudaError_t launch_fill_q32(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st);
 
 }  // namespace gsj

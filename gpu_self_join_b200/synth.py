@@ -47,9 +47,9 @@ class Workload:
 WORKLOADS = {
     "c1_uniform2d": Workload("c1_uniform2d", 0, 100_000, 2, 1.0, 32.4, 2, True, False, 0, False, False),
     "c2_gmm2d": Workload("c2_gmm2d", 1, 20_000_000, 2, 0.24630223214626312, 32.0, 2, True, False, 0, False, False),
-    "c3_gmm6d": Workload("c3_gmm6d", 2, 5_000_000, 6, 0.0, 64.0, 6, True, False, 0, False, False),
-    "c4_derived18d": Workload("c4_derived18d", 3, 5_000_000, 18, 0.0, 100.0, 6, False, True, 8, True, True),
-    "c5_heavy90d": Workload("c5_heavy90d", 4, 515_345, 90, 0.0, 50.0, 6, False, True, 8, True, True),
+    "c3_gmm6d": Workload("c3_gmm6d", 2, 5_000_000, 6, 2.0983946323394775, 64.0, 6, True, False, 0, False, False),
+    "c4_derived18d": Workload("c4_derived18d", 3, 5_000_000, 18, 0.4803199768066406, 100.0, 6, False, True, 8, True, True),
+    "c5_heavy90d": Workload("c5_heavy90d", 4, 515_345, 90, 13.249305725097656, 50.0, 6, False, True, 8, True, True),
 }
 
 
