@@ -61,6 +61,7 @@ class GsjStats(ctypes.Structure):
         ("dev_ms_count", ctypes.c_double),
         ("dev_ms_fill", ctypes.c_double),
         ("kernel_launches", ctypes.c_uint64),
+        ("join_path", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

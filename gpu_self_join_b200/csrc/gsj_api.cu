@@ -23,6 +23,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -141,7 +142,7 @@ struct gsj_context {
     Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
         item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
-        minmax_part;
+        minmax_part, pairs, pairs2;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
     // last result
@@ -299,6 +300,105 @@ int validate(gsj_context* c, const gsj_config& cfg, uint64_t N) {
     if (cfg.ilp > (uint32_t)kMaxIlp) return fail(c, GSJ_ERR_INVALID, "ILP above 64 is not supported");
     if (cfg.dtype != GSJ_FLOAT32 && cfg.dtype != GSJ_FLOAT64) return fail(c, GSJ_ERR_INVALID, "unknown dtype");
     if (N >= (1ull << 31)) return fail(c, GSJ_ERR_INVALID, "at most 2^31-1 points per join");
+    return GSJ_OK;
+}
+
+// ------------------------------------------------------------------ tile join
+// Count, pair buffer, sort and table of the tile join (high-dimensional float
+// data).  A sampling pass over every kSampleStride-th item sizes the pair
+// buffer; the full pass counts every pair even past the buffer, so a short
+// buffer is re-sized to the exact count and the pass repeated.
+int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int model, uint32_t* counts,
+              uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
+    constexpr uint32_t kSampleStride = 64;
+    gsj_stats& S = c->stats;
+    cudaStream_t st = c->st;
+    uint32_t shift = 1;
+    while (shift < 32 && ((N - 1) >> shift)) shift++;
+    const uint32_t ni = a.num_items;
+    TileOut o{};
+    o.cursor = cursor;
+    o.shift = shift;
+    unsigned long long* cand = reinterpret_cast<unsigned long long*>(a.work_counter + 2);
+    auto reset = [&]() -> int {
+        // work counter, error flag and candidate statistic, then the cursor
+        GSJ_CUDA(c, cudaMemsetAsync(a.work_counter, 0, 4 * sizeof(uint32_t), st));
+        GSJ_CUDA(c, cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
+        return GSJ_OK;
+    };
+    GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
+    // ---- sampling pass
+    const uint32_t nsample = (ni + kSampleStride - 1) / kSampleStride;
+    GSJ_TRY(reset());
+    o.emit = false;
+    o.stride = kSampleStride;
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_tile_join(a, o, stamp, model, nsample, c->num_sms, st));
+    unsigned long long sampled = 0;
+    GSJ_TRY(d2h_small(c, &sampled, cursor, 1));
+    const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
+    uint64_t cap = (uint64_t)(est * 1.25) + N + (1u << 16);
+    // ---- full pass (repeated once with the exact size if the buffer was short)
+    unsigned long long* pairs = nullptr;
+    unsigned long long R = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        GSJ_TRY(dev_get(c, c->pairs, cap, &pairs));
+        GSJ_TRY(reset());
+        o.emit = true;
+        o.stride = 1;
+        o.pairs = pairs;
+        o.cap = cap;
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_tile_join(a, o, stamp, model, ni, c->num_sms, st));
+        GSJ_TRY(d2h_small(c, &R, cursor, 1));
+        if (R <= cap) break;
+        if (attempt == 1) return fail(c, GSJ_ERR_STATE, "tile join: pair count changed between two passes");
+        cap = R;
+    }
+    GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
+    // ---- on-device pair sort -> neighbour table in point-id order
+    GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
+    unsigned long long* sorted = nullptr;
+    uint32_t* table = nullptr;
+    GSJ_TRY(dev_get(c, c->pairs2, R ? R : 1, &sorted));
+    GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
+    GSJ_CUDA(c, cudaMemsetAsync(counts, 0, (N + 1) * sizeof(uint32_t), st));
+    if (R) {
+        size_t tb = 0;
+        void* temp = nullptr;
+        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, tb, pairs, sorted, (uint64_t)R, 0, (int)(2 * shift), st));
+        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(temp, tb, pairs, sorted, (uint64_t)R, 0, (int)(2 * shift), st));
+        S.kernel_launches += 2 * shift / 8 + 2;
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_pairs_to_table(sorted, R, shift, table, counts, c->num_sms, st));
+    }
+    void* stemp = nullptr;
+    GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
+    S.kernel_launches += 3;
+    GSJ_CUDA(c, scan_u32_u64(counts, offsets, N, stemp, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
+    uint64_t total = 0;
+    GSJ_TRY(d2h_small(c, &total, offsets + N, 1));
+    if (total != R) return fail(c, GSJ_ERR_STATE, "tile join: list lengths disagree with the pair count");
+    unsigned long long ncand = 0;
+    GSJ_TRY(d2h_small(c, &ncand, cand, 1));
+    {
+        float ms = 0;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
+        S.dev_ms_index = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[2], c->tev[3]));
+        S.dev_ms_count = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[4], c->tev[5]));
+        S.dev_ms_fill = ms;
+    }
+    S.candidates = ncand;
+    S.join_path = GSJ_PATH_TILE;
+    S.ms_join = now_ms() - t_join;
+    S.total_pairs = R;
+    c->R = R;
+    c->have_result = true;
+    S.ms_total = now_ms() - t_start;
     return GSJ_OK;
 }
 
@@ -495,6 +595,15 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_CUDA(c, launch_slot_cell(cell_start, M, slot_cell, st));
     }
 
+    // High-dimensional float data with populated cells (at least 8 points per
+    // non-empty cell on average) takes the tile join; everything else the
+    // warp-per-item passes.
+    const int model = model_of(cfg);
+    bool tile = false;
+    if constexpr (std::is_same<T, float>::value)
+        tile = tile_supported(n, npad, k, model, cfg.ilp) && N >= 8ull * M;
+    const uint32_t qchunk = tile ? (uint32_t)kTileQ : (uint32_t)kQChunk;
+
     // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525)
     uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
     GSJ_TRY(dev_get(c, c->nchunks, M + 1, &nchunks));
@@ -506,7 +615,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_TRY(dev_get(c, c->order, 2 * (size_t)M, &order));
         iota = order + M;
         S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, nchunks, sizes, st));
+    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, sizes, st));
         S.kernel_launches += 1;
     GSJ_CUDA(c, launch_iota(iota, M, st));
         // stable descending sort by cell size: ties keep ascending cell order
@@ -516,10 +625,10 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_CUDA(c, cub::DeviceRadixSort::SortPairsDescending(temp, tb, sizes, sizes2, iota, order, (int)M, 0, 32,
                                                               st));
         S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_item_counts(cell_start, order, M, nchunks, nullptr, st));
+    GSJ_CUDA(c, launch_item_counts(cell_start, order, M, qchunk, nchunks, nullptr, st));
     } else {
         S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, nchunks, nullptr, st));
+    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, nullptr, st));
     }
     GSJ_CUDA(c, cudaMemsetAsync(nchunks + M, 0, sizeof(uint32_t), st));
     GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tb, nchunks, item_off, (int)M + 1, st));
@@ -570,8 +679,13 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.fwd_cnt = fwd;
     a.rev_cnt = rev;
     a.cand_cnt = cand;
-    const int model = model_of(cfg);
     const bool stamp = cfg.stamp != 0 && !(cfg.flags & GSJ_FLAG_NO_UNICOMP);
+    if constexpr (std::is_same<T, float>::value) {
+        if (tile) {
+            unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
+            return tile_join(c, a, N, stamp, model, counts, offsets, cursor, t_join, t_start);
+        }
+    }
     // On the row-range path the distance work is cheap, so the fill pass walks
     // the full neighbourhood and writes every list forward only (contiguous,
     // deterministic); the count pass keeps the unicomp traversal of STAMP.  The
@@ -636,6 +750,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     if (errflag) return fail(c, GSJ_ERR_STATE, "fill pass disagreed with the count pass (table bound reached)");
     S.ms_join = now_ms() - t_join;
     S.total_pairs = R;
+    S.join_path = tpq ? GSJ_PATH_ROWS : GSJ_PATH_WARP;
     c->R = R;
     c->have_result = true;
     S.ms_total = now_ms() - t_start;
@@ -724,7 +839,7 @@ int gsj_destroy(gsj_context* c) {
                    &c->order,    &c->sizes,
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
                    &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
-                   &c->minarr,   &c->minmax_part};
+                   &c->minarr,   &c->minmax_part, &c->pairs, &c->pairs2};
     for (Buf* b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})

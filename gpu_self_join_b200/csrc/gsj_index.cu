@@ -224,14 +224,15 @@ __global__ void k_cell_plan(const uint64_t* __restrict__ cell_key, uint32_t M, G
 }
 
 // ------------------------------------------------------------ work items
-// A work item is one chunk of up to kQChunk consecutive query slots of one cell.
+// A work item is one chunk of up to `qchunk` consecutive query slots of one cell.
 __global__ void k_item_counts(const uint32_t* __restrict__ cell_start, const uint32_t* __restrict__ order,
-                              uint32_t M, uint32_t* __restrict__ nchunks, uint32_t* __restrict__ sizes) {
+                              uint32_t M, uint32_t qchunk, uint32_t* __restrict__ nchunks,
+                              uint32_t* __restrict__ sizes) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= M) return;
     const uint32_t c = order ? order[i] : i;
     const uint32_t sz = cell_start[c + 1] - cell_start[c];
-    nchunks[i] = (sz + kQChunk - 1) / kQChunk;
+    nchunks[i] = (sz + qchunk - 1) / qchunk;
     if (sizes) sizes[i] = sz;
 }
 
@@ -311,9 +312,9 @@ cudaError_t launch_cell_plan(const uint64_t* cell_key, uint32_t M, const GridGeo
     return cudaGetLastError();
 }
 
-cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t* nchunks,
-                               uint32_t* sizes, cudaStream_t st) {
-    k_item_counts<<<blocks_for(M, 256), 256, 0, st>>>(cell_start, order, M, nchunks, sizes);
+cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t qchunk,
+                               uint32_t* nchunks, uint32_t* sizes, cudaStream_t st) {
+    k_item_counts<<<blocks_for(M, 256), 256, 0, st>>>(cell_start, order, M, qchunk, nchunks, sizes);
     return cudaGetLastError();
 }
 

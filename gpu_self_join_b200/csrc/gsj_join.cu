@@ -65,30 +65,6 @@ __host__ __device__ inline WarpSmem warp_smem_layout(uint32_t npad, uint32_t tsi
     return w;
 }
 
-// Slot range of the cell with linear id `lin`: from the dense slot-prefix
-// table (ds[lin] .. ds[lin+1]) or through the hash table of non-empty cells.
-template <typename T>
-__device__ __forceinline__ bool lookup_range(const JoinArgs<T>& a, uint64_t lin, uint32_t& start, uint32_t& cnt) {
-    if (a.ds) {
-        start = a.ds[lin];
-        cnt = a.ds[lin + 1] - start;
-        return cnt != 0;
-    }
-    uint64_t h = mix64(lin) & a.hmask;
-    for (uint64_t p = 0; p <= a.hmask; p++) {
-        const uint64_t kk = a.hkeys[h];
-        if (kk == lin) {
-            const uint32_t c = a.hvals[h];
-            start = a.cell_start[c];
-            cnt = a.cell_start[c + 1] - start;
-            return true;
-        }
-        if (kk == kEmptyKey) return false;
-        h = (h + 1) & a.hmask;
-    }
-    return false;
-}
-
 template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS, bool ROWS>
 __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff,
                                               uint32_t batch) {

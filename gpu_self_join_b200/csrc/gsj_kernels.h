@@ -28,8 +28,8 @@ cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, c
                                uint64_t hmask, cudaStream_t st);
 cudaError_t launch_cell_plan(const uint64_t* cell_key, uint32_t M, const GridGeom& g, const uint32_t* ds,
                              uint2* plan, uint8_t* par, cudaStream_t st);
-cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t* nchunks,
-                               uint32_t* sizes, cudaStream_t st);
+cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t qchunk,
+                               uint32_t* nchunks, uint32_t* sizes, cudaStream_t st);
 cudaError_t launch_make_items(const uint32_t* order, const uint32_t* nchunks, const uint32_t* item_off,
                               uint32_t M, uint2* items, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st);
@@ -54,5 +54,26 @@ cudaError_t launch_count_tpq(const JoinArgs<T>& a, const uint32_t* slot_cell, in
 // Fill pass of dense low-dimensional grids: a warp per 32 consecutive query slots.
 template <typename T>
 cudaError_t launch_fill_q32(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st);
+
+// Tile join of high-dimensional float data (5 <= n <= kTileMaxN, k <= 6):
+// a CTA per item of up to kTileQ query slots; hits become packed
+// (query id << shift | candidate id) keys in a pair buffer.
+constexpr int kTileQ = 64;            // queries per tile-join work item
+constexpr uint32_t kTileMaxN = 128;   // dimensions held in shared memory
+struct TileOut {
+    unsigned long long* pairs;    // [cap] packed pairs
+    unsigned long long cap;       // pairs beyond cap are counted, not written
+    unsigned long long* cursor;   // pairs found so far (zeroed by the caller)
+    uint32_t shift;               // bits of a point id
+    uint32_t stride;              // items visited: 0, stride, 2*stride, ...
+    bool emit;                    // false: count only (the sampling pass)
+};
+bool tile_supported(uint32_t n, uint32_t npad, uint32_t k, int model, uint32_t ilp);
+// Visits items 0, stride, ..., (nvisit-1)*stride; a.work_counter must be zero.
+cudaError_t launch_tile_join(const JoinArgs<float>& a, const TileOut& o, bool stamp, int model, uint32_t nvisit,
+                             int num_sms, cudaStream_t st);
+// Sorted packed pairs -> table (low bits) and counts[query] += pairs (counts zeroed by the caller).
+cudaError_t launch_pairs_to_table(const unsigned long long* keys, uint64_t R, uint32_t shift, uint32_t* table,
+                                  uint32_t* counts, int num_sms, cudaStream_t st);
 
 }  // namespace gsj

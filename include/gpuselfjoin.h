@@ -83,10 +83,17 @@ typedef struct gsj_stats {
     double ms_total;          /* whole call                                     */
     /* device time (CUDA events on the context's stream) */
     double dev_ms_index;      /* index build: keys, sort, cells, lookup, items  */
-    double dev_ms_count;      /* count pass kernel                              */
-    double dev_ms_fill;       /* fill pass kernel                               */
+    double dev_ms_count;      /* count pass (tile join: the distance pass)      */
+    double dev_ms_fill;       /* fill pass (tile join: pair sort + table)       */
     uint64_t kernel_launches; /* launches of this library's own kernels         */
+    uint64_t join_path;       /* GSJ_PATH_* taken by the last join              */
 } gsj_stats;
+
+/* Join paths (gsj_stats.join_path). */
+#define GSJ_PATH_WARP 0u  /* warp per (cell, 32 queries): count pass + fill pass   */
+#define GSJ_PATH_ROWS 1u  /* dense k <= 3, n <= 4: thread-per-query count + fill   */
+#define GSJ_PATH_TILE 2u  /* float, 5 <= n <= 128, k <= 6, >= 8 points per cell:
+                             64 x 64 register tiles, pair buffer, on-device sort */
 
 typedef struct gsj_context gsj_context;
 

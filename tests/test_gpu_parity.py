@@ -91,6 +91,81 @@ def test_configs_match_oracle(oracle, case):
     assert st["total_pairs"] > N  # more than the self pairs
 
 
+# Tile join (float, 5 <= n <= 128, k <= 6, populated cells): every distance
+# model with and without unicomp, ILP that does not divide n, the largest n.
+TILE_CASES = [
+    # n, k, reorder, ilp, sc, stamp, qr, N
+    (5, 5, False, 0, False, False, False, 20000),
+    (18, 6, True, 8, True, False, True, 20000),
+    (18, 6, True, 8, False, True, False, 20000),
+    (18, 6, False, 4, True, True, True, 20000),
+    (33, 4, False, 3, False, False, False, 12000),
+    (90, 6, True, 8, True, False, True, 8000),
+    (90, 6, True, 8, True, True, False, 8000),
+    (128, 6, False, 0, False, True, False, 6000),
+]
+
+
+def tile_points(n, N, eps, seed):
+    """Clusters that fill their cells (sigma 1 in six dims, 0.1 in the rest)
+    plus partners placed at distance eps, so many pairs sit on the boundary."""
+    rng = np.random.default_rng(seed)
+    sig = np.full(n, 0.1)
+    sig[: min(6, n)] = 1.0
+    nb = N // 2
+    centres = rng.uniform(0, 10, size=(4, n))
+    base = centres[rng.integers(0, 4, nb)] + rng.standard_normal((nb, n)) * sig
+    d = rng.standard_normal((N - nb, n))
+    d *= eps / np.linalg.norm(d, axis=1, keepdims=True)
+    partner = base[rng.integers(0, nb, N - nb)] + d
+    return np.concatenate([base, partner]).astype(np.float32)[rng.permutation(N)]
+
+
+@pytest.mark.parametrize("case", TILE_CASES, ids=[f"n{c[0]}k{c[1]}r{int(c[2])}i{c[3]}s{int(c[4])}u{int(c[5])}q{int(c[6])}"
+                                                  for c in TILE_CASES])
+def test_tile_join_matches_oracle(oracle, case):
+    n, k, reorder, ilp, sc, stamp, qr, N = case
+    eps = 3.0
+    pts = tile_points(n, N, eps, 2000 + n)
+    st = assert_same(oracle, pts, eps, indexed_dims=k, reorder=reorder, ilp=ilp, shortcircuit=sc, stamp=stamp,
+                     query_reorder=qr)
+    assert st["join_path"] == 2  # GSJ_PATH_TILE
+    assert st["total_pairs"] > N
+
+
+def test_tile_join_deterministic():
+    pts = tile_points(18, 20000, 3.0, 7)
+    c1, t1, s1 = run_gpu(pts, 3.0, indexed_dims=6, stamp=True)
+    c2, t2, _ = run_gpu(pts, 3.0, indexed_dims=6, stamp=True)
+    assert s1["join_path"] == 2
+    assert np.array_equal(c1, c2) and np.array_equal(t1, t2)
+    # lists come out of the pair sort ascending
+    starts = np.concatenate([[0], np.cumsum(c1.astype(np.int64))])
+    assert all(np.all(np.diff(t1[starts[i]:starts[i + 1]].astype(np.int64)) > 0) for i in range(0, c1.size, 97))
+
+
+@pytest.mark.parametrize("name", ["c4_derived18d", "c5_heavy90d"])
+def test_full_size_high_dim_sample(oracle, name):
+    """The 18-D and 90-D workloads at full size: per-query list lengths of a
+    seeded query sample equal the oracle's, lists are symmetric."""
+    w = synth.WORKLOADS[name]
+    pts = synth.generate(name)
+    c, t, st = run_gpu(pts, w.eps, indexed_dims=w.k, reorder=w.reorder, ilp=w.ilp, shortcircuit=w.shortcircuit,
+                       stamp=w.stamp, query_reorder=w.query_reorder)
+    assert st["join_path"] == 2
+    q = np.random.default_rng(11).choice(pts.shape[0], 150, replace=False).astype(np.uint32)
+    ocfg = oracle_cfg(oracle, w.k, w.reorder, w.ilp, w.shortcircuit)
+    total, _, _ = oracle.join_sample(pts, w.eps, ocfg, q)
+    assert int(c[q].astype(np.int64).sum()) == total
+    starts = np.concatenate([[0], np.cumsum(c.astype(np.int64))])
+    for i in q[:40]:
+        lst = t[starts[i]:starts[i + 1]]
+        assert i in lst
+        for j in lst[:: max(1, lst.size // 8)]:
+            lj = t[starts[j]:starts[j + 1]]
+            assert i in lj
+
+
 @pytest.mark.parametrize("stamp", [False, True])
 def test_dense_cell_many_chunks(oracle, stamp):
     # 3000 points in few cells: query cells span many 32-query chunks
