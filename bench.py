@@ -203,7 +203,7 @@ def _ours(args) -> None:
     pts = synth.generate(args.workload, args.points)
     N, n = pts.shape
     cfg = JoinConfig(indexed_dims=w.k, reorder=w.reorder, shortcircuit=w.shortcircuit, ilp=w.ilp, stamp=w.stamp,
-                     query_reorder=w.query_reorder)
+                     query_reorder=w.query_reorder, plain=args.plain)
     sj = SelfJoin(local_rank)
     x_dev = torch.from_numpy(pts).cuda()
     torch.cuda.synchronize()
@@ -297,9 +297,11 @@ def _ours(args) -> None:
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded, shapes/distributions of the benchmark workload)",
         "config": {"workload": args.workload, "points": N, "dim": n, "eps": w.eps, "indexed_dims": w.k,
+                   "plain": bool(args.plain),
                    "stamp": w.stamp, "reorder": w.reorder, "ilp": w.ilp, "shortcircuit": w.shortcircuit,
                    "query_reorder": w.query_reorder, "result_pairs_per_step": R,
-                   "candidates_per_step": stats[-1]["candidates"], "parallelism": f"replicas x{world}",
+                   "candidates_per_step": stats[-1]["candidates"], "join_path": int(stats[-1]["join_path"]),
+                   "screen_rechecks_per_step": int(stats[-1]["screen_rechecks"]), "parallelism": f"replicas x{world}",
                    "l2": "inputs (160 MB) and working set larger than L2"},
         "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
     }
@@ -365,6 +367,8 @@ def main():
                     help="generate a smaller instance of the workload (profiling captures only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true",
+                    help="no tensor-core screen on high-dimensional workloads (exact FP32 for every pair)")
     args = ap.parse_args()
     if args.impl == "reference":
         _reference_arm(args)

@@ -19,6 +19,7 @@ GSJ_FLOAT64 = 1
 GSJ_FLAG_SORT_LISTS = 0x1
 GSJ_FLAG_QUIET = 0x2
 GSJ_FLAG_NO_UNICOMP = 0x4
+GSJ_FLAG_PLAIN = 0x8
 
 # Every symbol declared in include/gpuselfjoin.h.
 EXPORTED_SYMBOLS = (
@@ -62,6 +63,7 @@ class GsjStats(ctypes.Structure):
         ("dev_ms_fill", ctypes.c_double),
         ("kernel_launches", ctypes.c_uint64),
         ("join_path", ctypes.c_uint64),
+        ("screen_rechecks", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

@@ -142,7 +142,7 @@ struct gsj_context {
     Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
         item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
-        minmax_part, pairs, pairs2;
+        minmax_part, pairs, pairs2, srows, snorms, spartial, scentre, unc;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
     // last result
@@ -308,8 +308,8 @@ int validate(gsj_context* c, const gsj_config& cfg, uint64_t N) {
 // data).  A sampling pass over every kSampleStride-th item sizes the pair
 // buffer; the full pass counts every pair even past the buffer, so a short
 // buffer is re-sized to the exact count and the pass repeated.
-int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int model, uint32_t* counts,
-              uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
+int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int model, bool screen,
+              uint32_t* counts, uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
     constexpr uint32_t kSampleStride = 64;
     gsj_stats& S = c->stats;
     cudaStream_t st = c->st;
@@ -319,41 +319,87 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
     TileOut o{};
     o.cursor = cursor;
     o.shift = shift;
+    o.rechecks = nullptr;
     unsigned long long* cand = reinterpret_cast<unsigned long long*>(a.work_counter + 2);
+    a.err_flag = a.work_counter + 1;
+    ScreenConst sc = make_screen_const(a.n, a.thr);
     auto reset = [&]() -> int {
-        // work counter, error flag and candidate statistic, then the cursor
+        // work counter, error flag and candidate statistic, then the cursor and rechecks
         GSJ_CUDA(c, cudaMemsetAsync(a.work_counter, 0, 4 * sizeof(uint32_t), st));
-        GSJ_CUDA(c, cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
+        GSJ_CUDA(c, cudaMemsetAsync(cursor, 0, 2 * sizeof(unsigned long long), st));
         return GSJ_OK;
     };
+    auto launch = [&](uint32_t nvisit) -> cudaError_t {
+        return screen ? launch_tile_screen(a, o, sc, stamp, model, nvisit, c->num_sms, st)
+                      : launch_tile_join(a, o, stamp, model, nvisit, c->num_sms, st);
+    };
     GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
+    if (screen) {
+        // centred BF16 rows and norms of all points, read by every candidate tile
+        uint4* rows = nullptr;
+        float *norms = nullptr, *centre = nullptr;
+        double* partial = nullptr;
+        GSJ_TRY(dev_get(c, c->srows, N * (sc.kpad / 8), &rows));
+        GSJ_TRY(dev_get(c, c->snorms, N, &norms));
+        GSJ_TRY(dev_get(c, c->spartial, (size_t)kScreenPrepBlocks * a.n, &partial));
+        GSJ_TRY(dev_get(c, c->scentre, a.n, &centre));
+        S.kernel_launches += 3;
+        GSJ_CUDA(c, launch_screen_prep(a.pts, (uint32_t)N, a.n, a.npad, sc.kpad, partial, centre, rows, norms, st));
+        sc.rows = rows;
+        sc.norms = norms;
+    }
     // ---- sampling pass
     const uint32_t nsample = (ni + kSampleStride - 1) / kSampleStride;
     GSJ_TRY(reset());
     o.emit = false;
     o.stride = kSampleStride;
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_tile_join(a, o, stamp, model, nsample, c->num_sms, st));
+    GSJ_CUDA(c, launch(nsample));
     unsigned long long sampled = 0;
     GSJ_TRY(d2h_small(c, &sampled, cursor, 1));
+    {
+        uint32_t err = 0;
+        GSJ_TRY(d2h_small(c, &err, a.err_flag, 1));
+        if (err) return fail(c, GSJ_ERR_CUDA, "tile join: tensor-core wait timed out");
+    }
     const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
     uint64_t cap = (uint64_t)(est * 1.25) + N + (1u << 16);
-    // ---- full pass (repeated once with the exact size if the buffer was short)
-    unsigned long long* pairs = nullptr;
-    unsigned long long R = 0;
+    // ---- full pass (repeated once with the exact size if the buffer was short):
+    // the tile join's hits, or the screen's undecided pairs
+    unsigned long long *list = nullptr, *pairs = nullptr;
+    unsigned long long U = 0, R = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
-        GSJ_TRY(dev_get(c, c->pairs, cap, &pairs));
+        GSJ_TRY(dev_get(c, screen ? c->unc : c->pairs, cap, &list));
         GSJ_TRY(reset());
         o.emit = true;
         o.stride = 1;
-        o.pairs = pairs;
+        o.pairs = list;
         o.cap = cap;
         S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_tile_join(a, o, stamp, model, ni, c->num_sms, st));
-        GSJ_TRY(d2h_small(c, &R, cursor, 1));
-        if (R <= cap) break;
+        GSJ_CUDA(c, launch(ni));
+        GSJ_TRY(d2h_small(c, &U, cursor, 1));
+        uint32_t err = 0;
+        GSJ_TRY(d2h_small(c, &err, a.err_flag, 1));
+        if (err) return fail(c, GSJ_ERR_CUDA, "tile join: tensor-core wait timed out");
+        if (U <= cap) break;
         if (attempt == 1) return fail(c, GSJ_ERR_STATE, "tile join: pair count changed between two passes");
-        cap = R;
+        cap = U;
+    }
+    if (screen) {
+        // exact check of the undecided pairs; each yields at most one pair, two with unicomp
+        const uint64_t pcap = stamp ? 2 * U : U;
+        GSJ_TRY(dev_get(c, c->pairs, pcap ? pcap : 1, &pairs));
+        GSJ_CUDA(c, cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), st));
+        TileOut ro = o;
+        ro.pairs = pairs;
+        ro.cap = pcap;
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_screen_recheck(a, list, U, ro, stamp, model, c->num_sms, st));
+        GSJ_TRY(d2h_small(c, &R, cursor, 1));
+        if (R > pcap) return fail(c, GSJ_ERR_STATE, "screened join: more pairs than undecided candidates");
+    } else {
+        pairs = list;
+        R = U;
     }
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
     // ---- on-device pair sort -> neighbour table in point-id order
@@ -393,7 +439,8 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         S.dev_ms_fill = ms;
     }
     S.candidates = ncand;
-    S.join_path = GSJ_PATH_TILE;
+    S.screen_rechecks = screen ? U : 0;
+    S.join_path = screen ? GSJ_PATH_SCREEN : GSJ_PATH_TILE;
     S.ms_join = now_ms() - t_join;
     S.total_pairs = R;
     c->R = R;
@@ -470,7 +517,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     const uint32_t nparts = (uint32_t)std::min<uint64_t>((N + 255) / 256, (uint64_t)c->num_sms * 4);
     T *d_part = nullptr, *d_mm = nullptr;
     GSJ_TRY(dev_get(c, c->minmax_part, (size_t)nparts * 2 * k, &d_part));
-    GSJ_TRY(dev_get(c, c->misc, 2 * kMaxK + 8, &d_mm));
+    GSJ_TRY(dev_get(c, c->misc, 2 * kMaxK + 16, &d_mm));
     S.kernel_launches += 2;
     GSJ_CUDA(c, launch_minmax<T>(d_in, N, n, k, d_perm, d_part, nparts, d_mm, st));
     std::vector<T> mm(2 * k);
@@ -598,11 +645,16 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     // High-dimensional float data with populated cells (at least 8 points per
     // non-empty cell on average) takes the tile join; everything else the
     // warp-per-item passes.
+    // From 16 dimensions on, the tile join screens pairs with BF16 dot
+    // products on the tensor cores (GSJ_FLAG_PLAIN turns the screen off).
     const int model = model_of(cfg);
-    bool tile = false;
-    if constexpr (std::is_same<T, float>::value)
+    bool tile = false, screen = false;
+    if constexpr (std::is_same<T, float>::value) {
         tile = tile_supported(n, npad, k, model, cfg.ilp) && N >= 8ull * M;
-    const uint32_t qchunk = tile ? (uint32_t)kTileQ : (uint32_t)kQChunk;
+        screen = tile && !(cfg.flags & GSJ_FLAG_PLAIN) &&
+                 screen_supported(n, npad, k, model, cfg.ilp, threshold_of<float>(eps));
+    }
+    const uint32_t qchunk = screen ? (uint32_t)kScreenQ : tile ? (uint32_t)kTileQ : (uint32_t)kQChunk;
 
     // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525)
     uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
@@ -683,7 +735,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     if constexpr (std::is_same<T, float>::value) {
         if (tile) {
             unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
-            return tile_join(c, a, N, stamp, model, counts, offsets, cursor, t_join, t_start);
+            return tile_join(c, a, N, stamp, model, screen, counts, offsets, cursor, t_join, t_start);
         }
     }
     // On the row-range path the distance work is cheap, so the fill pass walks
@@ -839,7 +891,8 @@ int gsj_destroy(gsj_context* c) {
                    &c->order,    &c->sizes,
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
                    &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
-                   &c->minarr,   &c->minmax_part, &c->pairs, &c->pairs2};
+                   &c->minarr,   &c->minmax_part, &c->pairs, &c->pairs2, &c->srows, &c->snorms,
+                   &c->spartial, &c->scentre, &c->unc};
     for (Buf* b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})

@@ -1,0 +1,760 @@
+// Tensor-core screened tile join for high-dimensional float data.
+//
+// Same work decomposition and output as the tile join (gsj_join_tile.cu): a
+// CTA owns up to kScreenQ = 128 consecutive query slots of one cell, walks the
+// concatenated candidate slots of the cell's neighbour cells (3^k offsets,
+// kernel.cu:180-303) 128 at a time and appends every pair within eps as a
+// packed (query id, candidate id) key.  What changes is how a pair is decided:
+//
+//   1. Once per join (k_screen_rows), every point is centred on the data mean
+//      o and rounded to BF16, c^ = bf16(fl(c - o)), and stored with its norm
+//      as a row [c^, |c^|^2_hi, |c^|^2_lo] (slot order).  Candidate tiles are
+//      copied from these rows (cp.async, 16-byte chunks) into K-major
+//      shared-memory tiles (8 x 16-byte core matrices, no swizzle); the query
+//      tile holds [-2 q^, 1, 1], so the product carries the candidate norm.
+//   2. One thread issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, M = N =
+//      128, K = 16 per instruction) over the padded dimensions; the 128 x 128
+//      values |c^_j|^2 - 2 q^_i.c^_j accumulate in tensor memory (exact
+//      BF16 products; -2 q^ is exact in BF16).
+//   3. Every consumer thread reads its query's row (tcgen05.ld 32x32b) and
+//      rejects candidate j when that value exceeds
+//      G_i = (R0 + kE (|q^_i| + max_j |c^_j|))^2 + c1 (|q^_i|^2 + 2 max_j |c^_j|^2) - |q^_i|^2.
+//      The bound is proven, not tuned: R0^2 covers the rounding of the
+//      reference's own FP32 sum (at most 2n+8 roundings of non-negative
+//      terms), kE the BF16 rounding of both centred points and of the centring
+//      (|x - bf16(x)| <= 2^-8 |x|), c1 the FP32 accumulation (K + 32 steps of
+//      2^-20) and the two-term BF16 split of the norm (2^-16).  A pair within
+//      eps by the reference's arithmetic is therefore never rejected.
+//   4. Every pair not rejected is appended to a list of undecided pairs;
+//      k_screen_recheck recomputes each in the reference's exact FP32 order
+//      from the original coordinates (ILP/SHORTCIRCUIT model,
+//      kernel.cu:307-365) and keeps it iff s <= thr.
+// The emitted pair set is the plain path's, bit for bit.  Non-finite values
+// only make the test inconclusive, which sends the pair to the exact check.
+//
+// Synchronisation: warps 4-7 produce candidate tiles (slot search, cp.async of
+// the rows) and issue the MMA, warps
+// 0-3 consume; two tiles and two accumulators alternate, handed over by
+// mbarriers (full: MMA commit + the issuer's release; empty: 128 consumer
+// arrivals).  Every wait is a bounded poll by one thread whose verdict is
+// shared before any barrier or warp-collective; on time-out the error flag is
+// raised and the CTA stops.  Tensor memory (2 x 128 columns) is allocated once
+// per CTA; the shared-memory request keeps at most 2 CTAs (512 columns) on an
+// SM; it is released before exit.
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "gsj_common.cuh"
+#include "gsj_fp.cuh"
+#include "gsj_kernels.h"
+
+namespace gsj {
+
+namespace {
+
+constexpr int kSQ = kScreenQ;        // queries per item = MMA M
+constexpr int kSC = 128;             // candidates per tile = MMA N
+constexpr int kSThreads = 384;      // warps 0-7 consume, warps 8-11 produce
+constexpr int kProd0 = 256;         // first producer thread
+constexpr uint32_t kTmemCols = 128;  // FP32 accumulator columns (N)
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kMinSmem = 80u * 1024u;  // at most 2 CTAs (2 x 256 TMEM columns) per SM
+constexpr uint32_t kWaitPolls = 1u << 20;
+
+// Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bit 4),
+// A and B BF16 (bits 7 and 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kSC >> 3) << 17) |
+                            ((uint32_t)(kSQ >> 4) << 24);
+
+__device__ __forceinline__ unsigned lanemask_lt_s() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8 rows
+// x 16 bytes; LBO = byte distance between K-adjacent core matrices, SBO =
+// between row-group-adjacent ones; version 1 (bit 46).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)((lbo >> 4) & 0x3fffu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+}
+
+// Byte offset of element (r, k) of a K-major tile with kpad columns.
+__device__ __forceinline__ uint32_t core_off(uint32_t r, uint32_t kc, uint32_t kpad) {
+    return ((r >> 3) * (kpad >> 3) + kc) * 128u + (r & 7u) * 16u;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// try_wait suspends the thread in hardware until the phase completes or an
+// implementation-defined time passes; the loop bounds the total wait.
+__device__ __forceinline__ bool bar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool bar_wait_bounded(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kWaitPolls; it++)
+        if (bar_try(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// The reference's squared distance in its exact order, one thread, stopping
+// as soon as the running value (which only grows) is above thr.
+template <int MODEL>
+__device__ float exact_sqdist(const float* __restrict__ q, const float* __restrict__ c, uint32_t n, uint32_t ilp,
+                              float thr) {
+    if (MODEL == kSeq || MODEL == kIlpSc) {
+        float s = 0.f;
+        uint32_t p = 0;
+        for (uint32_t l = 0; l < n; l++) {
+            const float d = __fsub_rn(c[l], q[l]);
+            s = (MODEL == kSeq || p == 0) ? __fmaf_rn(d, d, s) : __fadd_rn(s, __fmaf_rn(d, d, 0.f));
+            if (MODEL == kIlpSc && ++p == ilp) p = 0;
+            if (s > thr) break;
+        }
+        return s;
+    } else {
+        float s = 0.f;
+        for (uint32_t j = 0; j < ilp && j < n; j++) {
+            float r = 0.f;
+            for (uint32_t l = j; l < n; l += ilp) {
+                const float d = __fsub_rn(c[l], q[l]);
+                r = __fmaf_rn(d, d, r);
+            }
+            s = j == 0 ? r : __fadd_rn(s, r);
+            if (s > thr) break;
+        }
+        return s;
+    }
+}
+
+// Same arithmetic, rows read as float4 blocks of 32 dimensions loaded before
+// use (npad is a multiple of 4 here); the ILP model without SHORTCIRCUIT
+// walks its dimensions with stride ILP and keeps the scalar form.
+template <int MODEL>
+__device__ float exact_sqdist4(const float* __restrict__ q, const float* __restrict__ c, uint32_t n, uint32_t ilp,
+                               float thr) {
+    if (MODEL == kIlp) return exact_sqdist<MODEL>(q, c, n, ilp, thr);
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    const float4* c4 = reinterpret_cast<const float4*>(c);
+    float s = 0.f;
+    uint32_t p = 0;
+    for (uint32_t l0 = 0; l0 < n; l0 += 32u) {
+        float4 qa[8], ca[8];
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            if (l0 + 4u * b < n) {
+                qa[b] = q4[(l0 >> 2) + b];
+                ca[b] = c4[(l0 >> 2) + b];
+            } else {
+                qa[b] = ca[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const float qv[4] = {qa[b].x, qa[b].y, qa[b].z, qa[b].w};
+            const float cv[4] = {ca[b].x, ca[b].y, ca[b].z, ca[b].w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                if (l0 + 4u * b + (uint32_t)e < n) {
+                    const float d = __fsub_rn(cv[e], qv[e]);
+                    s = (MODEL == kSeq || p == 0) ? __fmaf_rn(d, d, s) : __fadd_rn(s, __fmaf_rn(d, d, 0.f));
+                    if (MODEL == kIlpSc && ++p == ilp) p = 0;
+                }
+            }
+        }
+        if (s > thr) break;
+    }
+    return s;
+}
+
+struct ScreenSmem {
+    uint32_t a, b0, b1, nbs, nbp, cslot, cwmax, qid, qinfo, misc, total;
+};
+
+__host__ __device__ inline ScreenSmem screen_smem(uint32_t kpad, uint32_t noff) {
+    ScreenSmem t{};
+    uint32_t o = 0;
+    t.a = o;
+    o += (uint32_t)kSQ * kpad * 2u;
+    t.b0 = o;
+    o += (uint32_t)kSC * kpad * 2u;
+    t.b1 = o;
+    o += (uint32_t)kSC * kpad * 2u;
+    t.nbs = o;
+    o += noff * 4u;
+    t.nbp = o;
+    o += (noff + 1u) * 4u;
+    o = (o + 15u) & ~15u;
+    t.cslot = o;  // [2][kSC]
+    o += 2u * kSC * 4u;
+    t.cwmax = o;  // [2][4] largest candidate norm per producer warp
+    o += 8u * 4u;
+    t.qid = o;
+    o += kSQ * 4u;
+    o = (o + 15u) & ~15u;
+    t.qinfo = o;  // float4 per query: |q^|^2, R0 + kE |q^|, c1 |q^|^2, valid
+    o += kSQ * 16u;
+    t.misc = o;   // [0] item [1] failed [2] total [3] producers' wait verdict [4] tmem [8..19] warp counts
+                  // [24..31] mbarriers full0 full1 empty0 empty1
+    o += 32u * 4u;
+    t.total = (o + 127u) & ~127u;
+    return t;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void named_sync(uint32_t id, uint32_t count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// The CTA is warp-specialised: warps 4-7 produce (candidate slots, centred
+// BF16 candidate tile with the norm folded in, the MMA), warps 0-3 consume
+// (tensor-memory rows, the screen, the exact check, the pair appends).  Two
+// candidate tiles and two accumulators alternate; mbarriers full[s] (MMA done)
+// and empty[s] (accumulator read) hand them over.
+//
+// With the norm folded into the product (A row = [q^, 1, 1], B row =
+// [-2 c^, |c^|^2_hi, |c^|^2_lo]), the accumulator holds |c^_j|^2 - 2 q^_i.c^_j
+// directly and the screen is one comparison per pair.
+template <int MODEL, bool STAMP>
+__global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<float> a, const TileOut o,
+                                                              const ScreenConst sc, uint32_t noff, uint32_t nvisit) {
+    extern __shared__ __align__(1024) unsigned char ssm[];
+    const uint32_t n = a.n, npad = a.npad, k = a.g.k, kpad = sc.kpad;
+    const ScreenSmem L = screen_smem(kpad, noff);
+    unsigned char* A = ssm + L.a;
+    uint32_t* nb_start = reinterpret_cast<uint32_t*>(ssm + L.nbs);
+    uint32_t* nb_pref = reinterpret_cast<uint32_t*>(ssm + L.nbp);
+    uint32_t* c_slot = reinterpret_cast<uint32_t*>(ssm + L.cslot);
+    float* cwmax = reinterpret_cast<float*>(ssm + L.cwmax);
+    uint32_t* q_id = reinterpret_cast<uint32_t*>(ssm + L.qid);
+    float4* qinfo = reinterpret_cast<float4*>(ssm + L.qinfo);
+    uint32_t* misc = reinterpret_cast<uint32_t*>(ssm + L.misc);
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned lt = lanemask_lt_s();
+    const uint32_t sbo = (kpad >> 3) * 128u;
+    const uint32_t a_addr = smem_u32(A);
+    const uint32_t full0 = smem_u32(misc + 24), full1 = smem_u32(misc + 26);
+    const uint32_t empty0 = smem_u32(misc + 28), empty1 = smem_u32(misc + 30);
+
+    // ---- set-up: mbarriers, tensor memory (two accumulators)
+    if (tid == 0) {
+        misc[1] = 0u;
+        // full[s]: the MMA's commit + the issuing thread's release of the tile's metadata
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(full0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(full1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(empty0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(empty1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(misc + 4)),
+                     "r"(2u * kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = misc[4];
+    uint32_t tiles_done = 0;  // tiles of earlier items (the mbarrier phases)
+    unsigned long long cand_total = 0;
+
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) misc[0] = atomicAdd(a.work_counter, 1u);
+        __syncthreads();
+        const uint32_t vi = misc[0];
+        if (vi >= nvisit || misc[1]) break;
+        const uint2 wi = a.items[(size_t)vi * o.stride];
+        const uint32_t cell = wi.x;
+        const uint32_t cs0 = a.cell_start[cell], ce = a.cell_start[cell + 1];
+        const uint32_t q0 = cs0 + wi.y * (uint32_t)kSQ;
+        const uint32_t qn = min((uint32_t)kSQ, ce - q0);
+
+        // ---- neighbour cells in offset order (as the tile join)
+        uint32_t own[kMaxK];
+#pragma unroll
+        for (int j = 0; j < kMaxK; j++)
+            own[j] = (j < (int)k) ? FP<float>::to_uint_rz(FP<float>::div(
+                                        FP<float>::sub(a.pts[(size_t)cs0 * npad + j], a.minv[j]), a.eps))
+                                  : 0u;
+        uint32_t nnb = 0;
+        for (uint32_t base = 0; base < noff; base += kSThreads) {
+            const uint32_t off = base + tid;
+            bool ok = off < noff;
+            uint64_t lin = 0;
+            bool moved = false, hd_odd = false;
+            uint32_t t = off;
+#pragma unroll
+            for (int j = 0; j < kMaxK; j++) {
+                if (j < (int)k) {
+                    const int dl = (int)(t % 3u) - 1;
+                    t /= 3u;
+                    const long long nbj = (long long)own[j] + dl;
+                    if (nbj < 0 || nbj >= (long long)a.g.ncells[j]) ok = false;
+                    lin += (uint64_t)nbj * a.g.mult[j];
+                    if (dl != 0) {
+                        moved = true;
+                        hd_odd = (own[j] & 1u) != 0;
+                    }
+                }
+            }
+            if (STAMP && moved && !hd_odd) ok = false;
+            uint32_t st = 0, cnt = 0;
+            const bool found = ok && lookup_range(a, lin, st, cnt);
+            const unsigned m = __ballot_sync(FULL, found);
+            if (lane == 0) misc[8 + warp] = __popc(m);
+            __syncthreads();
+            uint32_t before = 0, all = 0;
+#pragma unroll
+            for (int w = 0; w < kSThreads / 32; w++) {
+                const uint32_t cw = misc[8 + w];
+                before += (w < warp) ? cw : 0u;
+                all += cw;
+            }
+            if (found) {
+                const uint32_t pos = nnb + before + __popc(m & lt);
+                nb_start[pos] = st;
+                nb_pref[pos] = cnt;
+            }
+            nnb += all;
+            __syncthreads();
+        }
+        if (warp == 0) {
+            uint32_t run = 0;
+            for (uint32_t b0 = 0; b0 < nnb; b0 += 32) {
+                const uint32_t i = b0 + lane;
+                const uint32_t v = i < nnb ? nb_pref[i] : 0u;
+                uint32_t x = v;
+#pragma unroll
+                for (int s = 1; s < 32; s <<= 1) {
+                    const uint32_t y = __shfl_up_sync(FULL, x, s);
+                    if (lane >= s) x += y;
+                }
+                if (i < nnb) nb_pref[i] = run + x - v;
+                run += __shfl_sync(FULL, x, 31);
+            }
+            if (lane == 0) {
+                nb_pref[nnb] = run;
+                misc[2] = run;
+            }
+        }
+        // ---- query tile [-2 q^, 1, 1] from the precomputed rows [q^, |q^|^2_hi, |q^|^2_lo]
+        const uint32_t kch = kpad >> 3;  // 16-byte chunks per row
+        if (tid < kSQ) {
+            const bool valid = (uint32_t)tid < qn;
+            q_id[tid] = valid ? a.ids[q0 + tid] : 0u;
+            const float nrm = valid ? sc.norms[q0 + tid] : 0.f;
+            qinfo[tid] = make_float4(nrm, __fmaf_ru(sc.ke, __fsqrt_ru(nrm), sc.r0), __fmul_ru(sc.c1, nrm),
+                                     valid ? 1.f : 0.f);
+        }
+        for (uint32_t e = tid; e < (uint32_t)kSQ * kch; e += kSThreads) {
+            const uint32_t r = e / kch, kc = e - r * kch;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r < qn) v = sc.rows[(size_t)(q0 + r) * kch + kc];
+            uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                __nv_bfloat162 b = *reinterpret_cast<__nv_bfloat162*>(&w[h]);
+                float2 f = __bfloat1622float2(b);
+                const uint32_t col = kc * 8u + 2u * (uint32_t)h;
+                f.x = col < n ? -2.f * f.x : (col < n + 2u && r < qn ? 1.f : 0.f);
+                f.y = col + 1u < n ? -2.f * f.y : (col + 1u < n + 2u && r < qn ? 1.f : 0.f);
+                b = __floats2bfloat162_rn(f.x, f.y);
+                w[h] = *reinterpret_cast<uint32_t*>(&b);
+            }
+            *reinterpret_cast<uint4*>(A + core_off(r, kc, kpad)) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        fence_async_smem();
+        __syncthreads();
+        const uint32_t total = misc[2];
+        const uint32_t T = (total + kSC - 1u) / kSC;
+        cand_total += (unsigned long long)total * qn;
+
+        if (tid >= kProd0) {
+            // ================= producer warps
+            const uint32_t pt = (uint32_t)tid - (uint32_t)kProd0;  // candidate row of the tile
+            for (uint32_t t = 0; t < T; t++) {
+                const uint32_t g = tiles_done + t, s = g & 1u;
+                unsigned char* B = ssm + (s ? L.b1 : L.b0);
+                if (g >= 2) {
+                    // one thread waits; the verdict reaches all producers through a barrier
+                    if (pt == 0) {
+                        const bool ok = bar_wait_bounded((s ? empty1 : empty0), ((g >> 1) - 1u) & 1u);
+                        misc[3] = ok ? 0u : 1u;
+                        if (!ok) misc[1] = 1u;
+                    }
+                    named_sync(1, 128);
+                    if (misc[3]) break;
+                }
+                const uint32_t f = t * kSC + pt;
+                uint32_t slot = kNone;
+                if (f < total) {
+                    uint32_t lo = 0, hi = nnb;
+                    while (hi - lo > 1) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (nb_pref[mid] <= f) lo = mid;
+                        else hi = mid;
+                    }
+                    slot = nb_start[lo] + (f - nb_pref[lo]);
+                }
+                c_slot[s * kSC + pt] = slot;
+                const bool valid = slot != kNone;
+                {
+                    const uint4* src = sc.rows + (size_t)(valid ? slot : 0u) * kch;
+                    const uint32_t dst = smem_u32(B);
+                    for (uint32_t kc = 0; kc < kch; kc++) cp_async16(dst + core_off(pt, kc, kpad), src + kc, valid ? 16u : 0u);
+                }
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                // the row's norm from its own copy (hi + lo, within 2^-16 of |c^|^2; the
+                // bound takes it 2^-14 larger)
+                float wm = 0.f;
+                if (valid) {
+                    const uint32_t cn = n, cn1 = n + 1u;
+                    const float hi = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(
+                        B + core_off(pt, cn >> 3, kpad) + (cn & 7u) * 2u));
+                    const float lo = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(
+                        B + core_off(pt, cn1 >> 3, kpad) + (cn1 & 7u) * 2u));
+                    wm = __fmul_ru(__fadd_ru(hi, fabsf(lo)), 1.0f + 0x1p-14f);
+                }
+#pragma unroll
+                for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
+                if (lane == 0) cwmax[s * 4u + (uint32_t)(warp - 8)] = wm;
+                fence_async_smem();
+                named_sync(1, 128);
+                if (pt == 0) {
+                    fence_after();
+                    const uint32_t b_addr = smem_u32(B);
+                    for (uint32_t ks = 0; ks < (kpad >> 4); ks++)
+                        mma_bf16(tmem + s * kTmemCols, smem_desc(a_addr + ks * 256u, 128u, sbo),
+                                 smem_desc(b_addr + ks * 256u, 128u, sbo), ks > 0 ? 1u : 0u);
+                    mma_commit((s ? full1 : full0));
+                    bar_arrive((s ? full1 : full0));
+                }
+            }
+        } else {
+            // ================= consumer warps: query row i = TMEM lane i; warps w and
+            // w + 4 share lane quarter w % 4 and split the columns
+            const uint32_t quarter = (uint32_t)warp & 3u, colbase = ((uint32_t)warp >> 2) * ((uint32_t)kSC / 2u);
+            const uint32_t i = quarter * 32u + (uint32_t)lane;
+            const float4 qi = qinfo[i];
+            const bool qvalid = qi.w != 0.f;
+            for (uint32_t t = 0; t < T; t++) {
+                const uint32_t g = tiles_done + t, s = g & 1u;
+                bool ok = true;
+                if (lane == 0) ok = bar_wait_bounded((s ? full1 : full0), (g >> 1) & 1u);
+                ok = __shfl_sync(FULL, ok ? 1u : 0u, 0) != 0u;
+                if (!ok) {
+                    misc[1] = 1u;
+                    break;
+                }
+                fence_after();
+                const float cmax = fmaxf(fmaxf(cwmax[s * 4u], cwmax[s * 4u + 1u]),
+                                         fmaxf(cwmax[s * 4u + 2u], cwmax[s * 4u + 3u]));
+                // G_i from the tile's largest candidate norm (an upper bound of every column's bound)
+                const float tt = __fmaf_ru(sc.ke, __fsqrt_ru(cmax), qi.y);
+                const float G =
+                    __fsub_ru(__fmaf_ru(tt, tt, __fadd_ru(qi.z, __fmul_ru(sc.c1, __fmul_ru(2.f, cmax)))), qi.x);
+                const uint32_t nvalid = min((uint32_t)kSC, total - t * kSC);
+                for (uint32_t col0 = colbase; col0 < colbase + (uint32_t)kSC / 2u; col0 += 16u) {
+                    float d[16];
+                    tmem_ld16(tmem + s * kTmemCols + ((quarter * 32u) << 16) + col0, d);
+                    unsigned und = 0;
+                    if (qvalid) {
+#pragma unroll
+                        for (int jj = 0; jj < 16; jj++) und |= (d[jj] > G) ? 0u : (1u << jj);
+                        if (col0 + 16u > nvalid) und &= (col0 >= nvalid) ? 0u : ((1u << (nvalid - col0)) - 1u);
+                    }
+                    if (!__any_sync(FULL, und != 0u)) continue;
+                    // the undecided pairs (query slot | cross << 31, candidate slot) go to
+                    // the exact check (k_screen_recheck), one atomic per warp and chunk
+                    const uint32_t nu = (uint32_t)__popc(und);
+                    uint32_t x = nu;
+#pragma unroll
+                    for (int sh = 1; sh < 32; sh <<= 1) {
+                        const uint32_t y = __shfl_up_sync(FULL, x, sh);
+                        if (lane >= sh) x += y;
+                    }
+                    const uint32_t wtotal = __shfl_sync(FULL, x, 31);
+                    unsigned long long base = 0;
+                    if (lane == 31) base = atomicAdd(o.cursor, (unsigned long long)wtotal);
+                    base = __shfl_sync(FULL, base, 31);
+                    if (o.emit) {
+                        unsigned long long p = base + (x - nu);
+                        const unsigned long long qword = (unsigned long long)(q0 + i);
+                        unsigned uu = und;
+                        while (uu) {
+                            const int b = __ffs(uu) - 1;
+                            uu &= uu - 1u;
+                            const uint32_t sl = c_slot[s * kSC + col0 + (uint32_t)b];
+                            const unsigned long long cr = (STAMP && (sl < cs0 || sl >= ce)) ? (1ull << 31) : 0ull;
+                            if (p < o.cap) o.pairs[p] = ((qword | cr) << 32) | sl;
+                            p++;
+                        }
+                    }
+                }
+                fence_before();
+                bar_arrive((s ? empty1 : empty0));
+            }
+        }
+        tiles_done += T;
+    }
+    // ---- tear-down: every MMA this CTA issued has been waited for (the last
+    // tiles by the epilogue), unless a wait timed out
+    if (misc[1] && tid == 0) *a.err_flag = 2u;
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2u * kTmemCols)
+                     : "memory");
+    if (tid == 0 && o.emit && cand_total) atomicAdd(a.cand_cnt, cand_total);
+}
+
+template <int MODEL, bool STAMP>
+cudaError_t launch_screen_one(const JoinArgs<float>& a, const TileOut& o, const ScreenConst& sc, uint32_t noff,
+                              uint32_t nvisit, int num_sms, cudaStream_t st) {
+    auto kern = k_tile_screen<MODEL, STAMP>;
+    const ScreenSmem L = screen_smem(sc.kpad, noff);
+    const uint32_t smem = L.total > kMinSmem ? L.total : kMinSmem;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSThreads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if ((uint32_t)per_sm * 2u * kTmemCols > 512u) return cudaErrorInvalidConfiguration;
+    uint64_t blocks = (uint64_t)num_sms * per_sm;
+    if (blocks > nvisit) blocks = nvisit ? nvisit : 1;
+    kern<<<(unsigned)blocks, kSThreads, smem, st>>>(a, o, sc, noff, nvisit);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// The exact check of the pairs the screen could not reject: the reference's
+// arithmetic for the configured model (kernel.cu:307-365), s <= thr; a hit
+// appends (query id, candidate id), and with the cross flag (unicomp, the
+// candidate outside the query's cell) also the reverse pair.
+template <int MODEL, bool STAMP>
+__global__ void __launch_bounds__(256) k_screen_recheck(const float* __restrict__ pts, const uint32_t* __restrict__ ids,
+                                                        uint32_t n, uint32_t npad, uint32_t ilp, float thr,
+                                                        const unsigned long long* __restrict__ unc,
+                                                        unsigned long long nunc, const TileOut o) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lt = lanemask_lt_s();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < nunc; i0 += stride) {
+        const uint64_t e = i0 + threadIdx.x;
+        bool hit = false, cross = false;
+        uint32_t qs = 0, cs = 0;
+        if (e < nunc) {
+            const unsigned long long w = unc[e];
+            cs = (uint32_t)w;
+            const uint32_t qw = (uint32_t)(w >> 32);
+            qs = qw & 0x7fffffffu;
+            const float d = exact_sqdist4<MODEL>(pts + (size_t)qs * npad, pts + (size_t)cs * npad, n, ilp, thr);
+            hit = d <= thr;
+            cross = STAMP && hit && (qw >> 31) != 0u;
+        }
+        const unsigned hb = __ballot_sync(FULL, hit), cb = __ballot_sync(FULL, cross);
+        if (hb == 0u) continue;
+        const uint32_t wtotal = (uint32_t)__popc(hb) + (uint32_t)__popc(cb);
+        unsigned long long base = 0;
+        if ((threadIdx.x & 31u) == 0u) base = atomicAdd(o.cursor, (unsigned long long)wtotal);
+        base = __shfl_sync(FULL, base, 0);
+        if (hit) {
+            unsigned long long p = base + (unsigned)__popc(hb & lt) + (unsigned)__popc(cb & lt);
+            const uint64_t qid = ids[qs], cid = ids[cs];
+            if (p < o.cap) o.pairs[p] = (qid << o.shift) | cid;
+            p++;
+            if (cross && p < o.cap) o.pairs[p] = (cid << o.shift) | qid;
+        }
+    }
+}
+
+template <int MODEL, bool STAMP>
+cudaError_t launch_recheck_one(const JoinArgs<float>& a, const unsigned long long* unc, unsigned long long nunc,
+                               const TileOut& o, int num_sms, cudaStream_t st) {
+    uint64_t blocks = (nunc + 255) / 256;
+    const uint64_t cap = (uint64_t)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    k_screen_recheck<MODEL, STAMP><<<(unsigned)blocks, 256, 0, st>>>(a.pts, a.ids, a.n, a.npad, a.ilp, a.thr, unc, nunc,
+                                                                     o);
+    return cudaGetLastError();
+}
+
+// Per-block FP64 column sums over a fixed row range (deterministic).
+__global__ void k_col_partial(const float* __restrict__ pts, uint32_t N, uint32_t n, uint32_t npad,
+                              double* __restrict__ partial) {
+    const uint32_t per = (N + gridDim.x - 1) / gridDim.x;
+    const uint32_t r0 = blockIdx.x * per, r1 = min(N, r0 + per);
+    for (uint32_t d = threadIdx.x; d < n; d += blockDim.x) {
+        double acc = 0.0;
+        for (uint32_t r = r0; r < r1; r++) acc += (double)pts[(size_t)r * npad + d];
+        partial[(size_t)blockIdx.x * n + d] = acc;
+    }
+}
+
+__global__ void k_col_mean(const double* __restrict__ partial, uint32_t nblocks, uint32_t N, uint32_t n,
+                           float* __restrict__ centre) {
+    for (uint32_t d = threadIdx.x; d < n; d += blockDim.x) {
+        double acc = 0.0;
+        for (uint32_t b = 0; b < nblocks; b++) acc += partial[(size_t)b * n + d];
+        centre[d] = N ? (float)(acc / (double)N) : 0.f;
+    }
+}
+
+// Row s: x' = fl(x - centre), c^ = bf16(x'), |c^|^2 in FP32 (sequential
+// fused sum of the exact squares), split into two BF16 terms.
+__global__ void k_screen_rows(const float* __restrict__ pts, uint32_t N, uint32_t n, uint32_t npad, uint32_t kpad,
+                              const float* __restrict__ centre, uint4* __restrict__ rows, float* __restrict__ norms) {
+    const uint32_t kch = kpad >> 3;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x) {
+        const float* x = pts + (size_t)s * npad;
+        float nrm = 0.f;
+        for (uint32_t kc = 0; kc < kch; kc++) {
+            uint32_t w[4];
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const uint32_t l = kc * 8u + 2u * (uint32_t)h;
+                const float x0 = l < n ? __fsub_rn(x[l], centre[l]) : 0.f;
+                const float x1 = l + 1u < n ? __fsub_rn(x[l + 1u], centre[l + 1u]) : 0.f;
+                const __nv_bfloat162 b = __floats2bfloat162_rn(x0, x1);
+                const float2 f = __bfloat1622float2(b);
+                nrm = __fmaf_rn(f.x, f.x, nrm);
+                nrm = __fmaf_rn(f.y, f.y, nrm);
+                w[h] = *reinterpret_cast<const uint32_t*>(&b);
+            }
+            rows[(size_t)s * kch + kc] = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        // the norm terms go to columns n and n + 1
+        const __nv_bfloat16 hi = __float2bfloat16_rn(nrm);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(__fsub_rn(nrm, __bfloat162float(hi)));
+        __nv_bfloat16* rb = reinterpret_cast<__nv_bfloat16*>(rows + (size_t)s * kch);
+        rb[n] = hi;
+        rb[n + 1u] = lo;
+        norms[s] = nrm;
+    }
+}
+
+cudaError_t launch_screen_prep(const float* pts, uint32_t N, uint32_t n, uint32_t npad, uint32_t kpad,
+                               double* partial, float* centre, uint4* rows, float* norms, cudaStream_t st) {
+    if (N == 0) return cudaSuccess;
+    if (kpad < n + 2u || (kpad & 7u)) return cudaErrorInvalidValue;
+    k_col_partial<<<kScreenPrepBlocks, 128, 0, st>>>(pts, N, n, npad, partial);
+    k_col_mean<<<1, 128, 0, st>>>(partial, kScreenPrepBlocks, N, n, centre);
+    uint64_t blocks = ((uint64_t)N + 255) / 256;
+    if (blocks > 148u * 16u) blocks = 148u * 16u;
+    k_screen_rows<<<(unsigned)blocks, 256, 0, st>>>(pts, N, n, npad, kpad, centre, rows, norms);
+    return cudaGetLastError();
+}
+
+bool screen_supported(uint32_t n, uint32_t npad, uint32_t k, int model, uint32_t ilp, float thr) {
+    // n + 2 columns: the dimensions and the folded candidate norm
+    return tile_supported(n, npad, k, model, ilp) && n >= 16 && n + 2u <= kTileMaxN && thr >= 1e-30f &&
+           thr <= 1e30f;
+}
+
+ScreenConst make_screen_const(uint32_t n, float thr) {
+    ScreenConst sc{};
+    sc.kpad = (n + 2u + 15u) & ~15u;
+    // R0 >= sqrt(thr / (1 - (2n + 8) 2^-24)), plus room for the FP32 evaluation of G
+    const double r0 = std::sqrt((double)thr) * (1.0 + (2.0 * n + 8.0) * 0x1p-24 + 0x1p-19);
+    sc.r0 = std::nextafter((float)r0, INFINITY);
+    // BF16 rounding of a centred coordinate: |x - bf16(x)| <= 2^-8 |x|, plus
+    // the centring subtraction and the square root of the norm
+    sc.ke = 0x1p-8f * 1.0045f;
+    // FP32 accumulation (K + 32 steps of 2^-20) and the two-term split of the
+    // folded candidate norm (2^-16)
+    sc.c1 = (float)(sc.kpad + 48u) * 0x1p-20f;
+    return sc;
+}
+
+cudaError_t launch_screen_recheck(const JoinArgs<float>& a, const unsigned long long* unc, unsigned long long nunc,
+                                  const TileOut& o, bool stamp, int model, int num_sms, cudaStream_t st) {
+    if (nunc == 0) return cudaSuccess;
+    if ((a.npad & 3u) || !unc) return cudaErrorInvalidValue;
+    switch (model * 2 + (stamp ? 1 : 0)) {
+        case kSeq * 2: return launch_recheck_one<kSeq, false>(a, unc, nunc, o, num_sms, st);
+        case kSeq * 2 + 1: return launch_recheck_one<kSeq, true>(a, unc, nunc, o, num_sms, st);
+        case kIlp * 2: return launch_recheck_one<kIlp, false>(a, unc, nunc, o, num_sms, st);
+        case kIlp * 2 + 1: return launch_recheck_one<kIlp, true>(a, unc, nunc, o, num_sms, st);
+        case kIlpSc * 2: return launch_recheck_one<kIlpSc, false>(a, unc, nunc, o, num_sms, st);
+        case kIlpSc * 2 + 1: return launch_recheck_one<kIlpSc, true>(a, unc, nunc, o, num_sms, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_tile_screen(const JoinArgs<float>& a, const TileOut& o, const ScreenConst& sc, bool stamp,
+                               int model, uint32_t nvisit, int num_sms, cudaStream_t st) {
+    if (!screen_supported(a.n, a.npad, a.g.k, model, a.ilp, a.thr) || o.stride == 0 || sc.kpad < a.n + 2u ||
+        !sc.rows || !sc.norms ||
+        (sc.kpad & 15u) || sc.kpad > kTileMaxN)
+        return cudaErrorInvalidValue;
+    if (nvisit == 0) return cudaSuccess;
+    if ((uint64_t)(nvisit - 1) * o.stride >= a.num_items) return cudaErrorInvalidValue;
+    uint32_t noff = 1;
+    for (uint32_t j = 0; j < a.g.k; j++) noff *= 3u;
+    switch (model * 2 + (stamp ? 1 : 0)) {
+        case kSeq * 2: return launch_screen_one<kSeq, false>(a, o, sc, noff, nvisit, num_sms, st);
+        case kSeq * 2 + 1: return launch_screen_one<kSeq, true>(a, o, sc, noff, nvisit, num_sms, st);
+        case kIlp * 2: return launch_screen_one<kIlp, false>(a, o, sc, noff, nvisit, num_sms, st);
+        case kIlp * 2 + 1: return launch_screen_one<kIlp, true>(a, o, sc, noff, nvisit, num_sms, st);
+        case kIlpSc * 2: return launch_screen_one<kIlpSc, false>(a, o, sc, noff, nvisit, num_sms, st);
+        case kIlpSc * 2 + 1: return launch_screen_one<kIlpSc, true>(a, o, sc, noff, nvisit, num_sms, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace gsj

@@ -67,6 +67,7 @@ struct TileOut {
     uint32_t shift;               // bits of a point id
     uint32_t stride;              // items visited: 0, stride, 2*stride, ...
     bool emit;                    // false: count only (the sampling pass)
+    unsigned long long* rechecks; // screened join: pairs sent to the exact check
 };
 bool tile_supported(uint32_t n, uint32_t npad, uint32_t k, int model, uint32_t ilp);
 // Visits items 0, stride, ..., (nvisit-1)*stride; a.work_counter must be zero.
@@ -75,5 +76,32 @@ cudaError_t launch_tile_join(const JoinArgs<float>& a, const TileOut& o, bool st
 // Sorted packed pairs -> table (low bits) and counts[query] += pairs (counts zeroed by the caller).
 cudaError_t launch_pairs_to_table(const unsigned long long* keys, uint64_t R, uint32_t shift, uint32_t* table,
                                   uint32_t* counts, int num_sms, cudaStream_t st);
+
+// Tensor-core screened tile join (gsj_join_screen.cu): BF16 tcgen05 dot
+// products with a proven rejection bound, exact FP32 check of the rest.
+constexpr int kScreenQ = 128;         // queries per screened work item (MMA M)
+struct ScreenConst {
+    float r0;             // >= sqrt(thr) with the reference sum's rounding room
+    float ke;             // BF16 rounding bound per unit norm
+    float c1;             // FP32 accumulation bound per unit squared norm
+    uint32_t kpad;        // dimensions + 2 padded to the MMA K step (16)
+    const uint4* rows;    // [N][kpad/8] centred BF16 rows [c^, |c^|^2_hi, |c^|^2_lo, 0...], slot order
+    const float* norms;   // [N] |c^|^2 (FP32 sum of the BF16 squares)
+};
+// Centred BF16 rows and norms of all points (slot order) for the screen:
+// centre = per-dimension mean (deterministic two-level FP64 sum); `partial`
+// holds kScreenPrepBlocks x n doubles, `centre` n floats.
+constexpr uint32_t kScreenPrepBlocks = 256;
+cudaError_t launch_screen_prep(const float* pts, uint32_t N, uint32_t n, uint32_t npad, uint32_t kpad,
+                               double* partial, float* centre, uint4* rows, float* norms, cudaStream_t st);
+bool screen_supported(uint32_t n, uint32_t npad, uint32_t k, int model, uint32_t ilp, float thr);
+ScreenConst make_screen_const(uint32_t n, float thr);
+// Screen pass: o.pairs / o.cursor receive the undecided pairs, packed as
+// (query slot | cross << 31) << 32 | candidate slot.
+cudaError_t launch_tile_screen(const JoinArgs<float>& a, const TileOut& o, const ScreenConst& sc, bool stamp,
+                               int model, uint32_t nvisit, int num_sms, cudaStream_t st);
+// Exact check of the undecided pairs; hits go to o as packed (query id, candidate id) keys.
+cudaError_t launch_screen_recheck(const JoinArgs<float>& a, const unsigned long long* unc, unsigned long long nunc,
+                                  const TileOut& o, bool stamp, int model, int num_sms, cudaStream_t st);
 
 }  // namespace gsj

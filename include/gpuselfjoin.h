@@ -49,6 +49,8 @@ extern "C" {
 #define GSJ_FLAG_QUIET      0x2u  /* no progress output on stdout              */
 #define GSJ_FLAG_NO_UNICOMP 0x4u  /* full neighbourhood traversal even with STAMP
                                      (same pair set, different work split)   */
+#define GSJ_FLAG_PLAIN      0x8u  /* no tensor-core screen: every candidate pair
+                                     is evaluated with the exact FP32 arithmetic */
 
 /*
  * Run-time configuration.  Field names follow params.h of the reference
@@ -87,6 +89,8 @@ typedef struct gsj_stats {
     double dev_ms_fill;       /* fill pass (tile join: pair sort + table)       */
     uint64_t kernel_launches; /* launches of this library's own kernels         */
     uint64_t join_path;       /* GSJ_PATH_* taken by the last join              */
+    uint64_t screen_rechecks; /* GSJ_PATH_SCREEN: pairs the BF16 screen could not
+                                 reject, evaluated exactly (0 on other paths)   */
 } gsj_stats;
 
 /* Join paths (gsj_stats.join_path). */
@@ -94,6 +98,9 @@ typedef struct gsj_stats {
 #define GSJ_PATH_ROWS 1u  /* dense k <= 3, n <= 4: thread-per-query count + fill   */
 #define GSJ_PATH_TILE 2u  /* float, 5 <= n <= 128, k <= 6, >= 8 points per cell:
                              64 x 64 register tiles, pair buffer, on-device sort */
+#define GSJ_PATH_SCREEN 3u /* float, 16 <= n <= 128, k <= 6, >= 8 points per cell:
+                             BF16 tcgen05 screen with a proven bound, exact FP32
+                             check of the rest, pair buffer, on-device sort   */
 
 typedef struct gsj_context gsj_context;
 

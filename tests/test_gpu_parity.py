@@ -121,23 +121,33 @@ def tile_points(n, N, eps, seed):
     return np.concatenate([base, partner]).astype(np.float32)[rng.permutation(N)]
 
 
+@pytest.mark.parametrize("plain", [False, True], ids=["screen", "plain"])
 @pytest.mark.parametrize("case", TILE_CASES, ids=[f"n{c[0]}k{c[1]}r{int(c[2])}i{c[3]}s{int(c[4])}u{int(c[5])}q{int(c[6])}"
                                                   for c in TILE_CASES])
-def test_tile_join_matches_oracle(oracle, case):
+def test_tile_join_matches_oracle(oracle, case, plain):
+    """Plain tile join and, from 16 dimensions on, the BF16 tensor-core
+    screen: both must give the oracle's lists exactly."""
     n, k, reorder, ilp, sc, stamp, qr, N = case
     eps = 3.0
     pts = tile_points(n, N, eps, 2000 + n)
     st = assert_same(oracle, pts, eps, indexed_dims=k, reorder=reorder, ilp=ilp, shortcircuit=sc, stamp=stamp,
-                     query_reorder=qr)
-    assert st["join_path"] == 2  # GSJ_PATH_TILE
+                     query_reorder=qr, plain=plain)
+    screened = 16 <= n <= 126 and not plain  # n + 2 columns (the folded norm) within 128
+    assert st["join_path"] == (3 if screened else 2)  # GSJ_PATH_SCREEN / GSJ_PATH_TILE
     assert st["total_pairs"] > N
+    if screened:
+        # every exact pair is among the rechecked ones; the screen rejects the rest
+        assert st["total_pairs"] <= 2 * st["screen_rechecks"]
+        assert st["screen_rechecks"] < st["candidates"]
 
 
 def test_tile_join_deterministic():
     pts = tile_points(18, 20000, 3.0, 7)
     c1, t1, s1 = run_gpu(pts, 3.0, indexed_dims=6, stamp=True)
     c2, t2, _ = run_gpu(pts, 3.0, indexed_dims=6, stamp=True)
-    assert s1["join_path"] == 2
+    c3, t3, s3 = run_gpu(pts, 3.0, indexed_dims=6, stamp=True, plain=True)
+    assert s1["join_path"] == 3 and s3["join_path"] == 2
+    assert np.array_equal(c1, c3) and np.array_equal(t1, t3)
     assert np.array_equal(c1, c2) and np.array_equal(t1, t2)
     # lists come out of the pair sort ascending
     starts = np.concatenate([[0], np.cumsum(c1.astype(np.int64))])
@@ -152,7 +162,7 @@ def test_full_size_high_dim_sample(oracle, name):
     pts = synth.generate(name)
     c, t, st = run_gpu(pts, w.eps, indexed_dims=w.k, reorder=w.reorder, ilp=w.ilp, shortcircuit=w.shortcircuit,
                        stamp=w.stamp, query_reorder=w.query_reorder)
-    assert st["join_path"] == 2
+    assert st["join_path"] == 3
     q = np.random.default_rng(11).choice(pts.shape[0], 150, replace=False).astype(np.uint32)
     ocfg = oracle_cfg(oracle, w.k, w.reorder, w.ilp, w.shortcircuit)
     total, _, _ = oracle.join_sample(pts, w.eps, ocfg, q)
