@@ -319,7 +319,9 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
     TileOut o{};
     o.cursor = cursor;
     o.shift = shift;
-    o.rechecks = nullptr;
+    o.rechecks = cursor + 1;  // the screen's exact count of undecided pairs
+    // entries the screen's consumer warps may leave unused: one block per warp
+    const uint64_t slack = screen ? (uint64_t)c->num_sms * 2u * 8u * kScreenBlockSlack : 0u;
     unsigned long long* cand = reinterpret_cast<unsigned long long*>(a.work_counter + 2);
     a.err_flag = a.work_counter + 1;
     ScreenConst sc = make_screen_const(a.n, a.thr);
@@ -356,18 +358,18 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
     S.kernel_launches += 1;
     GSJ_CUDA(c, launch(nsample));
     unsigned long long sampled = 0;
-    GSJ_TRY(d2h_small(c, &sampled, cursor, 1));
+    GSJ_TRY(d2h_small(c, &sampled, screen ? o.rechecks : cursor, 1));
     {
         uint32_t err = 0;
         GSJ_TRY(d2h_small(c, &err, a.err_flag, 1));
         if (err) return fail(c, GSJ_ERR_CUDA, "tile join: tensor-core wait timed out");
     }
     const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
-    uint64_t cap = (uint64_t)(est * 1.25) + N + (1u << 16);
+    uint64_t cap = (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
     // ---- full pass (repeated once with the exact size if the buffer was short):
     // the tile join's hits, or the screen's undecided pairs
     unsigned long long *list = nullptr, *pairs = nullptr;
-    unsigned long long U = 0, R = 0;
+    unsigned long long U = 0, R = 0, nlist = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         GSJ_TRY(dev_get(c, screen ? c->unc : c->pairs, cap, &list));
         GSJ_TRY(reset());
@@ -377,13 +379,19 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         o.cap = cap;
         S.kernel_launches += 1;
         GSJ_CUDA(c, launch(ni));
-        GSJ_TRY(d2h_small(c, &U, cursor, 1));
+        unsigned long long used = 0;  // entries written (pairs, or reserved undecided blocks)
+        GSJ_TRY(d2h_small(c, &used, cursor, 1));
+        U = used;
+        if (screen) GSJ_TRY(d2h_small(c, &U, o.rechecks, 1));
         uint32_t err = 0;
         GSJ_TRY(d2h_small(c, &err, a.err_flag, 1));
         if (err) return fail(c, GSJ_ERR_CUDA, "tile join: tensor-core wait timed out");
-        if (U <= cap) break;
+        if (used <= cap) {
+            nlist = used;
+            break;
+        }
         if (attempt == 1) return fail(c, GSJ_ERR_STATE, "tile join: pair count changed between two passes");
-        cap = U;
+        cap = U + slack;
     }
     if (screen) {
         // exact check of the undecided pairs; each yields at most one pair, two with unicomp
@@ -394,7 +402,7 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         ro.pairs = pairs;
         ro.cap = pcap;
         S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_screen_recheck(a, list, U, ro, stamp, model, c->num_sms, st));
+        GSJ_CUDA(c, launch_screen_recheck(a, list, nlist, ro, stamp, model, c->num_sms, st));
         GSJ_TRY(d2h_small(c, &R, cursor, 1));
         if (R > pcap) return fail(c, GSJ_ERR_STATE, "screened join: more pairs than undecided candidates");
     } else {

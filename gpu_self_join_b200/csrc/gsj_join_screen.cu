@@ -61,6 +61,7 @@ constexpr uint32_t kTmemCols = 128;  // FP32 accumulator columns (N)
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kMinSmem = 80u * 1024u;  // at most 2 CTAs (2 x 256 TMEM columns) per SM
 constexpr uint32_t kWaitPolls = 1u << 20;
+constexpr uint32_t kBlk = (uint32_t)kScreenBlockSlack;  // undecided-pair entries a consumer warp reserves
 
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bit 4),
 // A and B BF16 (bits 7 and 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
@@ -308,6 +309,9 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
     const uint32_t tmem = misc[4];
     uint32_t tiles_done = 0;  // tiles of earlier items (the mbarrier phases)
     unsigned long long cand_total = 0;
+    // consumer warps: the reserved block of undecided-pair entries and the count
+    unsigned long long blk_base = 0, und_count = 0;
+    uint32_t blk_used = kBlk;
 
     for (;;) {
         __syncthreads();
@@ -424,6 +428,9 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
         if (tid >= kProd0) {
             // ================= producer warps
             const uint32_t pt = (uint32_t)tid - (uint32_t)kProd0;  // candidate row of the tile
+            // the copy walks (row, chunk) pairs in row-major order, 128 apart
+            const uint32_t step_r = (uint32_t)kSC / kch, step_c = (uint32_t)kSC % kch;
+            uint32_t e = 0;  // neighbour range of this thread's current candidate (f grows by kSC per tile)
             for (uint32_t t = 0; t < T; t++) {
                 const uint32_t g = tiles_done + t, s = g & 1u;
                 unsigned char* B = ssm + (s ? L.b1 : L.b0);
@@ -439,37 +446,35 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 }
                 const uint32_t f = t * kSC + pt;
                 uint32_t slot = kNone;
+                float wm = 0.f;
                 if (f < total) {
-                    uint32_t lo = 0, hi = nnb;
-                    while (hi - lo > 1) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (nb_pref[mid] <= f) lo = mid;
-                        else hi = mid;
-                    }
-                    slot = nb_start[lo] + (f - nb_pref[lo]);
+                    while (nb_pref[e + 1] <= f) e++;
+                    slot = nb_start[e] + (f - nb_pref[e]);
+                    // |c^|^2 in FP32 bounds the folded hi + lo terms
+                    wm = sc.norms[slot];
                 }
                 c_slot[s * kSC + pt] = slot;
-                const bool valid = slot != kNone;
+                named_sync(1, 128);
                 {
-                    const uint4* src = sc.rows + (size_t)(valid ? slot : 0u) * kch;
                     const uint32_t dst = smem_u32(B);
-                    for (uint32_t kc = 0; kc < kch; kc++) cp_async16(dst + core_off(pt, kc, kpad), src + kc, valid ? 16u : 0u);
-                }
-                asm volatile("cp.async.wait_all;" ::: "memory");
-                // the row's norm from its own copy (hi + lo, within 2^-16 of |c^|^2; the
-                // bound takes it 2^-14 larger)
-                float wm = 0.f;
-                if (valid) {
-                    const uint32_t cn = n, cn1 = n + 1u;
-                    const float hi = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(
-                        B + core_off(pt, cn >> 3, kpad) + (cn & 7u) * 2u));
-                    const float lo = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(
-                        B + core_off(pt, cn1 >> 3, kpad) + (cn1 & 7u) * 2u));
-                    wm = __fmul_ru(__fadd_ru(hi, fabsf(lo)), 1.0f + 0x1p-14f);
+                    uint32_t r = pt / kch, kc = pt % kch;
+                    for (uint32_t j = 0; j < kch; j++) {
+                        const uint32_t sl = c_slot[s * kSC + r];
+                        const bool valid = sl != kNone;
+                        cp_async16(dst + core_off(r, kc, kpad), sc.rows + (size_t)(valid ? sl : 0u) * kch + kc,
+                                   valid ? 16u : 0u);
+                        r += step_r;
+                        kc += step_c;
+                        if (kc >= kch) {
+                            kc -= kch;
+                            r++;
+                        }
+                    }
                 }
 #pragma unroll
                 for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
                 if (lane == 0) cwmax[s * 4u + (uint32_t)(warp - 8)] = wm;
+                asm volatile("cp.async.wait_all;" ::: "memory");
                 fence_async_smem();
                 named_sync(1, 128);
                 if (pt == 0) {
@@ -526,11 +531,19 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                         if (lane >= sh) x += y;
                     }
                     const uint32_t wtotal = __shfl_sync(FULL, x, 31);
-                    unsigned long long base = 0;
-                    if (lane == 31) base = atomicAdd(o.cursor, (unsigned long long)wtotal);
-                    base = __shfl_sync(FULL, base, 31);
+                    und_count += wtotal;
                     if (o.emit) {
-                        unsigned long long p = base + (x - nu);
+                        if (blk_used + wtotal > kBlk) {
+                            // pad the rest of the warp's block, reserve the next one
+                            for (uint32_t e2 = blk_used + (uint32_t)lane; e2 < kBlk; e2 += 32u)
+                                if (blk_base + e2 < o.cap) o.pairs[blk_base + e2] = kUndecidedPad;
+                            unsigned long long nb = 0;
+                            if (lane == 0) nb = atomicAdd(o.cursor, (unsigned long long)kBlk);
+                            blk_base = __shfl_sync(FULL, nb, 0);
+                            blk_used = 0;
+                        }
+                        unsigned long long p = blk_base + blk_used + (x - nu);
+                        blk_used += wtotal;
                         const unsigned long long qword = (unsigned long long)(q0 + i);
                         unsigned uu = und;
                         while (uu) {
@@ -548,6 +561,13 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
             }
         }
         tiles_done += T;
+    }
+    // ---- the consumer warps' last blocks and their exact undecided counts
+    if (tid < kProd0) {
+        if (o.emit && blk_used < kBlk)
+            for (uint32_t e2 = blk_used + (uint32_t)lane; e2 < kBlk; e2 += 32u)
+                if (blk_base + e2 < o.cap) o.pairs[blk_base + e2] = kUndecidedPad;
+        if (lane == 0 && und_count) atomicAdd(o.rechecks, und_count);
     }
     // ---- tear-down: every MMA this CTA issued has been waited for (the last
     // tiles by the epilogue), unless a wait timed out
@@ -589,7 +609,7 @@ cudaError_t launch_screen_one(const JoinArgs<float>& a, const TileOut& o, const 
 template <int MODEL, bool STAMP>
 __global__ void __launch_bounds__(256) k_screen_recheck(const float* __restrict__ pts, const uint32_t* __restrict__ ids,
                                                         uint32_t n, uint32_t npad, uint32_t ilp, float thr,
-                                                        const unsigned long long* __restrict__ unc,
+                                                        uint32_t npoints, const unsigned long long* __restrict__ unc,
                                                         unsigned long long nunc, const TileOut o) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lt = lanemask_lt_s();
@@ -598,10 +618,10 @@ __global__ void __launch_bounds__(256) k_screen_recheck(const float* __restrict_
         const uint64_t e = i0 + threadIdx.x;
         bool hit = false, cross = false;
         uint32_t qs = 0, cs = 0;
-        if (e < nunc) {
-            const unsigned long long w = unc[e];
+        const unsigned long long w = e < nunc ? unc[e] : kUndecidedPad;
+        const uint32_t qw = (uint32_t)(w >> 32);
+        if (w != kUndecidedPad && (qw & 0x7fffffffu) < npoints && (uint32_t)w < npoints) {
             cs = (uint32_t)w;
-            const uint32_t qw = (uint32_t)(w >> 32);
             qs = qw & 0x7fffffffu;
             const float d = exact_sqdist4<MODEL>(pts + (size_t)qs * npad, pts + (size_t)cs * npad, n, ilp, thr);
             hit = d <= thr;
@@ -629,8 +649,8 @@ cudaError_t launch_recheck_one(const JoinArgs<float>& a, const unsigned long lon
     uint64_t blocks = (nunc + 255) / 256;
     const uint64_t cap = (uint64_t)num_sms * 16;
     if (blocks > cap) blocks = cap;
-    k_screen_recheck<MODEL, STAMP><<<(unsigned)blocks, 256, 0, st>>>(a.pts, a.ids, a.n, a.npad, a.ilp, a.thr, unc, nunc,
-                                                                     o);
+    k_screen_recheck<MODEL, STAMP><<<(unsigned)blocks, 256, 0, st>>>(a.pts, a.ids, a.n, a.npad, a.ilp, a.thr,
+                                                                     a.n_points, unc, nunc, o);
     return cudaGetLastError();
 }
 

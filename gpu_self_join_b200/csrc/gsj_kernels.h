@@ -96,8 +96,12 @@ cudaError_t launch_screen_prep(const float* pts, uint32_t N, uint32_t n, uint32_
                                double* partial, float* centre, uint4* rows, float* norms, cudaStream_t st);
 bool screen_supported(uint32_t n, uint32_t npad, uint32_t k, int model, uint32_t ilp, float thr);
 ScreenConst make_screen_const(uint32_t n, float thr);
-// Screen pass: o.pairs / o.cursor receive the undecided pairs, packed as
-// (query slot | cross << 31) << 32 | candidate slot.
+// Screen pass: the undecided pairs, packed as (query slot | cross << 31) << 32
+// | candidate slot, go to o.pairs in blocks that consumer warps reserve on
+// o.cursor (kScreenBlockSlack entries per warp at most stay unused, filled
+// with kUndecidedPad); o.rechecks receives their exact number.
+constexpr unsigned long long kUndecidedPad = ~0ull;
+constexpr uint64_t kScreenBlockSlack = 1024;
 cudaError_t launch_tile_screen(const JoinArgs<float>& a, const TileOut& o, const ScreenConst& sc, bool stamp,
                                int model, uint32_t nvisit, int num_sms, cudaStream_t st);
 // Exact check of the undecided pairs; hits go to o as packed (query id, candidate id) keys.
