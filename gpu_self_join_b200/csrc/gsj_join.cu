@@ -363,8 +363,12 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     const size_t smem = (size_t)warps * L.total;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    // the whole unified L1/shared array as shared memory, so that the CTAs the
+    // occupancy calculation counts on are resident together
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    e = blocks_per_sm((const void*)kern, threads, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     const uint64_t needed = ((uint64_t)a.num_items + warps - 1) / warps;

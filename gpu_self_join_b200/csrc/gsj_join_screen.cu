@@ -41,6 +41,7 @@
 // raised and the CTA stops.  Tensor memory (2 x 128 columns) is allocated once
 // per CTA; the shared-memory request keeps at most 2 CTAs (512 columns) on an
 // SM; it is released before exit.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -62,6 +63,7 @@ constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kMinSmem = 80u * 1024u;  // at most 2 CTAs (2 x 256 TMEM columns) per SM
 constexpr uint32_t kWaitPolls = 1u << 20;
 constexpr uint32_t kBlk = (uint32_t)kScreenBlockSlack;  // undecided-pair entries a consumer warp reserves
+constexpr uint32_t kStages = 3;     // candidate tiles in flight (the accumulators alternate in 2)
 
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bit 4),
 // A and B BF16 (bits 7 and 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
@@ -140,6 +142,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
 // The reference's squared distance in its exact order, one thread, stopping
 // as soon as the running value (which only grows) is above thr.
 template <int MODEL>
@@ -211,7 +228,7 @@ __device__ float exact_sqdist4(const float* __restrict__ q, const float* __restr
 }
 
 struct ScreenSmem {
-    uint32_t a, b0, b1, nbs, nbp, cslot, cwmax, qid, qinfo, misc, total;
+    uint32_t a, b, nbs, nbp, cslot, cwmax, qid, qinfo, misc, total;
 };
 
 __host__ __device__ inline ScreenSmem screen_smem(uint32_t kpad, uint32_t noff) {
@@ -219,27 +236,25 @@ __host__ __device__ inline ScreenSmem screen_smem(uint32_t kpad, uint32_t noff) 
     uint32_t o = 0;
     t.a = o;
     o += (uint32_t)kSQ * kpad * 2u;
-    t.b0 = o;
-    o += (uint32_t)kSC * kpad * 2u;
-    t.b1 = o;
-    o += (uint32_t)kSC * kpad * 2u;
+    t.b = o;  // kStages candidate tiles
+    o += kStages * (uint32_t)kSC * kpad * 2u;
     t.nbs = o;
     o += noff * 4u;
     t.nbp = o;
     o += (noff + 1u) * 4u;
     o = (o + 15u) & ~15u;
-    t.cslot = o;  // [2][kSC]
-    o += 2u * kSC * 4u;
-    t.cwmax = o;  // [2][4] largest candidate norm per producer warp
-    o += 8u * 4u;
+    t.cslot = o;  // [kStages][kSC]
+    o += kStages * kSC * 4u;
+    t.cwmax = o;  // [kStages][4] largest candidate norm per producer warp
+    o += kStages * 4u * 4u;
     t.qid = o;
     o += kSQ * 4u;
     o = (o + 15u) & ~15u;
     t.qinfo = o;  // float4 per query: |q^|^2, R0 + kE |q^|, c1 |q^|^2, valid
     o += kSQ * 16u;
-    t.misc = o;   // [0] item [1] failed [2] total [3] producers' wait verdict [4] tmem [8..19] warp counts
-                  // [24..31] mbarriers full0 full1 empty0 empty1
-    o += 32u * 4u;
+    t.misc = o;   // [0] item [1] failed [2] total [4] tmem [8..19] warp counts
+                  // [24..31] mbarriers full0 full1 empty0 empty1, [32..37] free0 free1 free2
+    o += 48u * 4u;
     t.total = (o + 127u) & ~127u;
     return t;
 }
@@ -254,6 +269,21 @@ __device__ __forceinline__ void bar_arrive(uint32_t bar) {
 
 __device__ __forceinline__ void named_sync(uint32_t id, uint32_t count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// Barrier among `count` threads that also returns the OR of their flags, so a
+// decision taken after it is the same in every participating thread.
+__device__ __forceinline__ bool named_sync_or(uint32_t id, uint32_t count, bool flag) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)flag), "r"(id), "r"(count)
+        : "memory");
+    return r != 0u;
 }
 
 // The CTA is warp-specialised: warps 4-7 produce (candidate slots, centred
@@ -286,6 +316,7 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
     const uint32_t a_addr = smem_u32(A);
     const uint32_t full0 = smem_u32(misc + 24), full1 = smem_u32(misc + 26);
     const uint32_t empty0 = smem_u32(misc + 28), empty1 = smem_u32(misc + 30);
+    const uint32_t free0 = smem_u32(misc + 32);  // free_b = free0 + 8 b
 
     // ---- set-up: mbarriers, tensor memory (two accumulators)
     if (tid == 0) {
@@ -295,6 +326,9 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(full1) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(empty0) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(empty1) : "memory");
+        // free[b]: the consumers are done with stage b (candidate tile, slots, norm bound)
+        for (uint32_t b = 0; b < kStages; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(free0 + 8u * b) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -426,24 +460,17 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
         cand_total += (unsigned long long)total * qn;
 
         if (tid >= kProd0) {
-            // ================= producer warps
+            // ================= producer warps: stage tile t + 1 (slots, cp.async of
+            // the rows) before completing tile t (copies landed, MMA issued)
             const uint32_t pt = (uint32_t)tid - (uint32_t)kProd0;  // candidate row of the tile
             // the copy walks (row, chunk) pairs in row-major order, 128 apart
             const uint32_t step_r = (uint32_t)kSC / kch, step_c = (uint32_t)kSC % kch;
             uint32_t e = 0;  // neighbour range of this thread's current candidate (f grows by kSC per tile)
-            for (uint32_t t = 0; t < T; t++) {
-                const uint32_t g = tiles_done + t, s = g & 1u;
-                unsigned char* B = ssm + (s ? L.b1 : L.b0);
-                if (g >= 2) {
-                    // one thread waits; the verdict reaches all producers through a barrier
-                    if (pt == 0) {
-                        const bool ok = bar_wait_bounded((s ? empty1 : empty0), ((g >> 1) - 1u) & 1u);
-                        misc[3] = ok ? 0u : 1u;
-                        if (!ok) misc[1] = 1u;
-                    }
-                    named_sync(1, 128);
-                    if (misc[3]) break;
-                }
+            auto prepare = [&](uint32_t t) -> bool {
+                const uint32_t g = tiles_done + t, b = g % kStages;
+                bool bad = false;
+                if (g >= kStages && pt == 0) bad = !bar_wait_bounded(free0 + 8u * b, ((g / kStages) - 1u) & 1u);
+                if (named_sync_or(1, 128, bad)) return false;
                 const uint32_t f = t * kSC + pt;
                 uint32_t slot = kNone;
                 float wm = 0.f;
@@ -453,13 +480,13 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                     // |c^|^2 in FP32 bounds the folded hi + lo terms
                     wm = sc.norms[slot];
                 }
-                c_slot[s * kSC + pt] = slot;
+                c_slot[b * kSC + pt] = slot;
                 named_sync(1, 128);
                 {
-                    const uint32_t dst = smem_u32(B);
+                    const uint32_t dst = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
                     uint32_t r = pt / kch, kc = pt % kch;
                     for (uint32_t j = 0; j < kch; j++) {
-                        const uint32_t sl = c_slot[s * kSC + r];
+                        const uint32_t sl = c_slot[b * kSC + r];
                         const bool valid = sl != kNone;
                         cp_async16(dst + core_off(r, kc, kpad), sc.rows + (size_t)(valid ? sl : 0u) * kch + kc,
                                    valid ? 16u : 0u);
@@ -470,23 +497,44 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                             r++;
                         }
                     }
+                    asm volatile("cp.async.commit_group;" ::: "memory");
                 }
 #pragma unroll
                 for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
-                if (lane == 0) cwmax[s * 4u + (uint32_t)(warp - 8)] = wm;
-                asm volatile("cp.async.wait_all;" ::: "memory");
+                if (lane == 0) cwmax[b * 4u + (uint32_t)(warp - 8)] = wm;
+                return true;
+            };
+            auto complete = [&](uint32_t t, bool next_pending) -> bool {
+                const uint32_t g = tiles_done + t, b = g % kStages, s = g & 1u;
+                if (next_pending) asm volatile("cp.async.wait_group 1;" ::: "memory");
+                else asm volatile("cp.async.wait_group 0;" ::: "memory");
                 fence_async_smem();
-                named_sync(1, 128);
+                bool bad = false;
+                if (g >= 2 && pt == 0) bad = !bar_wait_bounded((s ? empty1 : empty0), ((g >> 1) - 1u) & 1u);
+                if (named_sync_or(1, 128, bad)) return false;
                 if (pt == 0) {
+                    // the tile's largest candidate norm and its square root (rounded up), for all consumers
+                    const float cmax = fmaxf(fmaxf(cwmax[b * 4u], cwmax[b * 4u + 1u]),
+                                             fmaxf(cwmax[b * 4u + 2u], cwmax[b * 4u + 3u]));
+                    cwmax[b * 4u] = cmax;
+                    cwmax[b * 4u + 1u] = __fsqrt_ru(cmax);
                     fence_after();
-                    const uint32_t b_addr = smem_u32(B);
+                    const uint32_t b_addr = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
                     for (uint32_t ks = 0; ks < (kpad >> 4); ks++)
                         mma_bf16(tmem + s * kTmemCols, smem_desc(a_addr + ks * 256u, 128u, sbo),
                                  smem_desc(b_addr + ks * 256u, 128u, sbo), ks > 0 ? 1u : 0u);
                     mma_commit((s ? full1 : full0));
                     bar_arrive((s ? full1 : full0));
                 }
+                return true;
+            };
+            bool ok = T == 0 || prepare(0);
+            for (uint32_t t = 0; ok && t < T; t++) {
+                if (t + 1 < T) ok = prepare(t + 1);
+                if (ok) ok = complete(t, t + 1 < T);
             }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            if (!ok && pt == 0) misc[1] = 1u;
         } else {
             // ================= consumer warps: query row i = TMEM lane i; warps w and
             // w + 4 share lane quarter w % 4 and split the columns
@@ -504,20 +552,30 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                     break;
                 }
                 fence_after();
-                const float cmax = fmaxf(fmaxf(cwmax[s * 4u], cwmax[s * 4u + 1u]),
-                                         fmaxf(cwmax[s * 4u + 2u], cwmax[s * 4u + 3u]));
+                const uint32_t b = g % kStages;
+                const float cmax = cwmax[b * 4u], rcmax = cwmax[b * 4u + 1u];
                 // G_i from the tile's largest candidate norm (an upper bound of every column's bound)
-                const float tt = __fmaf_ru(sc.ke, __fsqrt_ru(cmax), qi.y);
+                const float tt = __fmaf_ru(sc.ke, rcmax, qi.y);
                 const float G =
                     __fsub_ru(__fmaf_ru(tt, tt, __fadd_ru(qi.z, __fmul_ru(sc.c1, __fmul_ru(2.f, cmax)))), qi.x);
                 const uint32_t nvalid = min((uint32_t)kSC, total - t * kSC);
-                for (uint32_t col0 = colbase; col0 < colbase + (uint32_t)kSC / 2u; col0 += 16u) {
-                    float d[16];
-                    tmem_ld16(tmem + s * kTmemCols + ((quarter * 32u) << 16) + col0, d);
+                // a warp whose 32 query rows are all empty still waits for every tile
+                // (its arrivals keep the phases of empty[] in order) but skips the work
+                const uint32_t col_end = (quarter * 32u < qn) ? colbase + (uint32_t)kSC / 2u : colbase;
+                for (uint32_t c32 = colbase; c32 < col_end; c32 += 32u) {
+                  float d32[32];
+                  tmem_ld32(tmem + s * kTmemCols + ((quarter * 32u) << 16) + c32, d32);
+                  // common case: every value of the 32 columns above G (NaN counts as undecided)
+                  bool all_out = true;
+#pragma unroll
+                  for (int jj = 0; jj < 32; jj++) all_out = all_out && (d32[jj] > G);
+                  if (__all_sync(FULL, !qvalid || all_out || c32 >= nvalid)) continue;
+                  for (uint32_t h16 = 0; h16 < 2u; h16++) {
+                    const uint32_t col0 = c32 + 16u * h16;
                     unsigned und = 0;
                     if (qvalid) {
 #pragma unroll
-                        for (int jj = 0; jj < 16; jj++) und |= (d[jj] > G) ? 0u : (1u << jj);
+                        for (int jj = 0; jj < 16; jj++) und |= (d32[16 * h16 + jj] > G) ? 0u : (1u << jj);
                         if (col0 + 16u > nvalid) und &= (col0 >= nvalid) ? 0u : ((1u << (nvalid - col0)) - 1u);
                     }
                     if (!__any_sync(FULL, und != 0u)) continue;
@@ -547,17 +605,19 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                         const unsigned long long qword = (unsigned long long)(q0 + i);
                         unsigned uu = und;
                         while (uu) {
-                            const int b = __ffs(uu) - 1;
+                            const int bb = __ffs(uu) - 1;
                             uu &= uu - 1u;
-                            const uint32_t sl = c_slot[s * kSC + col0 + (uint32_t)b];
+                            const uint32_t sl = c_slot[b * kSC + col0 + (uint32_t)bb];
                             const unsigned long long cr = (STAMP && (sl < cs0 || sl >= ce)) ? (1ull << 31) : 0ull;
                             if (p < o.cap) o.pairs[p] = ((qword | cr) << 32) | sl;
                             p++;
                         }
                     }
+                  }
                 }
                 fence_before();
                 bar_arrive((s ? empty1 : empty0));
+                bar_arrive(free0 + 8u * b);
             }
         }
         tiles_done += T;
@@ -589,11 +649,16 @@ cudaError_t launch_screen_one(const JoinArgs<float>& a, const TileOut& o, const 
     const uint32_t smem = L.total > kMinSmem ? L.total : kMinSmem;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    // the whole unified L1/shared array as shared memory, so that the CTAs the
+    // occupancy calculation counts on are resident together
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSThreads, smem);
+    e = blocks_per_sm((const void*)kern, kSThreads, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    if ((uint32_t)per_sm * 2u * kTmemCols > 512u) return cudaErrorInvalidConfiguration;
+    // tensor memory: 2 accumulators of 128 columns per CTA, 512 columns per SM
+    if ((uint32_t)per_sm * 2u * kTmemCols > 512u) per_sm = (int)(512u / (2u * kTmemCols));
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > nvisit) blocks = nvisit ? nvisit : 1;
     kern<<<(unsigned)blocks, kSThreads, smem, st>>>(a, o, sc, noff, nvisit);

@@ -357,8 +357,12 @@ cudaError_t launch_tile_one(const JoinArgs<float>& a, const TileOut& o, uint32_t
     const TileSmem L = tile_smem(a.npad, noff);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
     if (e != cudaSuccess) return e;
+    // the whole unified L1/shared array as shared memory, so that the CTAs the
+    // occupancy calculation counts on are resident together
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, L.total);
+    e = blocks_per_sm((const void*)kern, kThreads, L.total, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
