@@ -26,7 +26,7 @@ EXPORTED_SYMBOLS = (
     "gsj_default_config", "gsj_set_default_config", "gsj_create", "gsj_destroy", "gsj_join",
     "gsj_result_size", "gsj_result_counts", "gsj_result_table", "gsj_result_device", "gsj_last_error",
     "gsj_threshold_f32", "gsj_threshold_f64", "GDSJoinPy", "copyResultIntoPythonArray", "GDSJoinPy_f32",
-    "GDSJoinPy_f64", "copyResultIntoPythonArray64", "gsj_list_offsets_noalloc",
+    "GDSJoinPy_f64", "copyResultIntoPythonArray64", "gsj_list_offsets_noalloc", "gsj_bruteforce_count",
 )
 
 
@@ -106,6 +106,8 @@ def lib() -> ctypes.CDLL:
     L.GDSJoinPy_f64.argtypes = [P, ctypes.c_uint, ctypes.c_double, ctypes.c_uint, i32, P]
     L.copyResultIntoPythonArray64.argtypes = [P, u64]
     L.gsj_list_offsets_noalloc.argtypes = [P, u64, P, P]
+    L.gsj_bruteforce_count.argtypes = [P, P, u64, ctypes.c_double, ctypes.POINTER(GsjConfig), i32, P,
+                                       ctypes.POINTER(u64)]
     L.copyResultIntoPythonArray.argtypes = [P, ctypes.c_uint]
     L.copyResultIntoPythonArray.restype = None
     L.GDSJoinPy.restype = None

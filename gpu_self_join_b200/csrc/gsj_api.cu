@@ -29,6 +29,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_run_length_encode.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 
 #include "../../include/gpuselfjoin.h"
 #include "gsj_common.cuh"
@@ -142,7 +143,7 @@ struct gsj_context {
     Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
         item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
-        minmax_part, pairs, pairs2, srows, snorms, spartial, scentre, unc;
+        minmax_part, pairs, pairs2, srows, snorms, spartial, scentre, unc, table2;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
     // last result
@@ -808,6 +809,23 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     uint32_t errflag = 0;
     GSJ_TRY(d2h_small(c, &errflag, ctr + 1, 1));
     if (errflag) return fail(c, GSJ_ERR_STATE, "fill pass disagreed with the count pass (table bound reached)");
+    if ((cfg.flags & GSJ_FLAG_SORT_LISTS) && R > 1) {
+        // every list ascending: a segmented sort of the table over the list offsets
+        if (R > 0x7fffffffull || N > 0x7fffffffull)
+            return fail(c, GSJ_ERR_INVALID, "GSJ_FLAG_SORT_LISTS needs fewer than 2^31 result pairs on this path");
+        uint32_t* sorted = nullptr;
+        GSJ_TRY(dev_get(c, c->table2, R, &sorted));
+        size_t tb2 = 0;
+        GSJ_CUDA(c, cub::DeviceSegmentedSort::SortKeys(nullptr, tb2, table, sorted, (int)R, (int)N, offsets,
+                                                       offsets + 1, st));
+        void* temp2 = nullptr;
+        GSJ_TRY(dev_get(c, c->temp, tb2, (unsigned char**)&temp2));
+        GSJ_CUDA(c, cub::DeviceSegmentedSort::SortKeys(temp2, tb2, table, sorted, (int)R, (int)N, offsets,
+                                                       offsets + 1, st));
+        S.kernel_launches += 4;
+        GSJ_CUDA(c, cudaStreamSynchronize(st));
+        std::swap(c->table, c->table2);
+    }
     S.ms_join = now_ms() - t_join;
     S.total_pairs = R;
     S.join_path = tpq ? GSJ_PATH_ROWS : GSJ_PATH_WARP;
@@ -900,7 +918,7 @@ int gsj_destroy(gsj_context* c) {
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
                    &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
                    &c->minarr,   &c->minmax_part, &c->pairs, &c->pairs2, &c->srows, &c->snorms,
-                   &c->spartial, &c->scentre, &c->unc};
+                   &c->spartial, &c->scentre, &c->unc, &c->table2};
     for (Buf* b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})
@@ -926,6 +944,50 @@ int gsj_join(gsj_context* c, const void* data, uint64_t num_points, double eps, 
                                       : run_join<double>(c, data, num_points, eps, *cfg, data_on_device);
     if (stats) *stats = c->stats;
     return r;
+}
+
+int gsj_bruteforce_count(gsj_context* c, const void* data, uint64_t num_points, double eps, const gsj_config* cfg,
+                         int data_on_device, uint32_t* counts, uint64_t* total) {
+    if (!c || !cfg || !total) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (!data && num_points) return fail(c, GSJ_ERR_INVALID, "null data");
+    if (cfg->dim == 0 || cfg->dim > 4096) return fail(c, GSJ_ERR_INVALID, "dim must be in 1..4096");
+    if (cfg->dtype != GSJ_FLOAT32 && cfg->dtype != GSJ_FLOAT64) return fail(c, GSJ_ERR_INVALID, "unknown dtype");
+    if (num_points >= (1ull << 31)) return fail(c, GSJ_ERR_INVALID, "at most 2^31-1 points");
+    if (cfg->device != c->device) return fail(c, GSJ_ERR_INVALID, "config device differs from the context's device");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    *total = 0;
+    if (num_points == 0) return GSJ_OK;
+    const uint32_t n = cfg->dim, N = (uint32_t)num_points;
+    const size_t tsz = cfg->dtype == GSJ_FLOAT32 ? 4 : 8;
+    cudaStream_t st = c->st;
+    const void* d_pts = data;
+    if (!data_on_device) {
+        unsigned char* p = nullptr;
+        GSJ_TRY(dev_get(c, c->in, (size_t)N * n * tsz, &p));
+        GSJ_TRY(h2d_copy(c, p, data, (size_t)N * n * tsz));
+        d_pts = p;
+    }
+    uint32_t* d_counts = nullptr;
+    unsigned long long* d_total = nullptr;
+    GSJ_TRY(dev_get(c, c->counts, (size_t)N + 1, &d_counts));
+    GSJ_TRY(dev_get(c, c->misc, 2 * kMaxK + 16, reinterpret_cast<double**>(&d_total)));
+    GSJ_CUDA(c, cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), st));
+    if (cfg->dtype == GSJ_FLOAT32) {
+        const float e = (float)eps;
+        if (!(e >= 0.f)) return fail(c, GSJ_ERR_INVALID, "epsilon must be non-negative");
+        GSJ_CUDA(c, launch_bruteforce<float>(static_cast<const float*>(d_pts), N, n, threshold_of<float>(e), d_counts,
+                                             d_total, st));
+    } else {
+        if (!(eps >= 0.0)) return fail(c, GSJ_ERR_INVALID, "epsilon must be non-negative");
+        GSJ_CUDA(c, launch_bruteforce<double>(static_cast<const double*>(d_pts), N, n, threshold_of<double>(eps),
+                                              d_counts, d_total, st));
+    }
+    unsigned long long t = 0;
+    GSJ_TRY(d2h_small(c, &t, d_total, 1));
+    *total = t;
+    if (counts) GSJ_TRY(d2h_staged(c, counts, d_counts, (size_t)N * 4));
+    c->have_result = false;  // the context's result buffers were reused
+    return GSJ_OK;
 }
 
 int gsj_result_size(gsj_context* c, uint64_t* total) {

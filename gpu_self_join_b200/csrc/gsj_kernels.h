@@ -137,4 +137,10 @@ cudaError_t launch_tile_screen(const JoinArgs<float>& a, const TileOut& o, const
 cudaError_t launch_screen_recheck(const JoinArgs<float>& a, const unsigned long long* unc, unsigned long long nunc,
                                   const TileOut& o, bool stamp, int model, int num_sms, cudaStream_t st);
 
+// Brute-force neighbour counts over all N^2 pairs (the reference's algorithm
+// 1, kernel.cu:486-515) with the sequential model: counts[q] and the total.
+template <typename T>
+cudaError_t launch_bruteforce(const T* pts, uint32_t N, uint32_t n, T thr, uint32_t* counts,
+                              unsigned long long* total, cudaStream_t st);
+
 }  // namespace gsj

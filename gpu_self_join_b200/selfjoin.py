@@ -105,6 +105,24 @@ class SelfJoin:
         self.N, self.n = Np, n
         return st.as_dict()
 
+    def bruteforce(self, points, eps: float) -> tuple[np.ndarray, int]:
+        """Brute-force neighbour counts over all N^2 pairs (the reference's GPU
+        algorithm 1, kernel.cu:486-515): (counts per point, total).  Replaces
+        any join result held by this object."""
+        p = np.ascontiguousarray(points)
+        if p.dtype not in (np.float32, np.float64):
+            p = p.astype(np.float32)
+        if p.ndim != 2:
+            raise ValueError("points must be N x n")
+        Np, n = p.shape
+        c = self._cfg(n, p.dtype, JoinConfig(indexed_dims=min(6, n)))
+        counts = np.empty(Np, dtype=np.uint32)
+        total = ctypes.c_uint64()
+        N.check(self._L.gsj_bruteforce_count(self._ctx, p.ctypes.data, Np, float(eps), ctypes.byref(c), 0,
+                                             counts.ctypes.data, ctypes.byref(total)), self._ctx)
+        self.N = 0
+        return counts, int(total.value)
+
     def total_pairs(self) -> int:
         r = ctypes.c_uint64()
         N.check(self._L.gsj_result_size(self._ctx, ctypes.byref(r)), self._ctx)

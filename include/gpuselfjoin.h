@@ -45,7 +45,10 @@ extern "C" {
 #define GSJ_FLOAT64 1
 
 /* flags */
-#define GSJ_FLAG_SORT_LISTS 0x1u  /* sort every neighbour list ascending       */
+#define GSJ_FLAG_SORT_LISTS 0x1u  /* sort every neighbour list ascending (an
+                                     on-device segmented sort after the fill; the
+                                     tile and screen paths' lists are ascending
+                                     anyway); below 2^31 result pairs per join   */
 #define GSJ_FLAG_QUIET      0x2u  /* no progress output on stdout              */
 #define GSJ_FLAG_NO_UNICOMP 0x4u  /* full neighbourhood traversal even with STAMP
                                      (same pair set, different work split)   */
@@ -153,6 +156,17 @@ GSJ_API const char* gsj_last_error(gsj_context* ctx);
  * sqrt(s) <= eps of kernel.cu:361/364 is evaluated as s <= threshold. */
 GSJ_API float gsj_threshold_f32(float eps);
 GSJ_API double gsj_threshold_f64(double eps);
+
+/* Brute-force neighbour counts over all N^2 pairs, self pairs included: the
+ * reference's GPU algorithm 1 (kernelBruteForce, kernel.cu:486-515, via
+ * makeDistanceTableGPUBruteForce, GPU.cu:1285-1440), with its arithmetic
+ * (`runningDist += (c-q)*(c-q)` over the dimensions in order, sqrt <= eps).
+ * cfg supplies dim and dtype (the index switches do not apply).  counts
+ * (optional, host, uint32[N]) receives each point's count, total the sum.
+ * O(N^2 n) work: an exact-count judge for the grid join on small inputs. */
+GSJ_API int gsj_bruteforce_count(gsj_context* ctx, const void* data, uint64_t num_points, double eps,
+                                 const gsj_config* cfg, int data_on_device, uint32_t* counts,
+                                 uint64_t* total);
 
 /*
  * List offsets without allocating: d_offsets[i] = d_counts[0] + ... +

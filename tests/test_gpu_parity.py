@@ -213,6 +213,39 @@ def test_collinear_k1(oracle):
     assert_same(oracle, pts, 0.05, indexed_dims=1, stamp=True)
 
 
+@pytest.mark.parametrize("case", ["rows_2d_stamp", "warp_3d_f64"])
+def test_sort_lists_flag(case):
+    """GSJ_FLAG_SORT_LISTS: the same lists, each ascending."""
+    if case == "rows_2d_stamp":
+        pts = synth.generate("c1_uniform2d")
+        kw = dict(indexed_dims=2, stamp=True)
+        eps = 1.0
+    else:
+        pts = np.random.default_rng(12).uniform(0, 40, size=(30000, 3))
+        kw = dict(indexed_dims=3)
+        eps = 1.5
+    c0, t0, s0 = run_gpu(pts, eps, **kw)
+    c1, t1, s1 = run_gpu(pts, eps, sort_lists=True, **kw)
+    assert s1["join_path"] == s0["join_path"] and s0["join_path"] in (0, 1)
+    assert np.array_equal(c0, c1)
+    assert np.array_equal(t1, canon(c0, t0))
+
+
+@pytest.mark.parametrize("case", [(3, np.float32, 20000, 1.5), (5, np.float64, 6000, 2.0), (90, np.float32, 3000, 20.0)])
+def test_bruteforce_matches_oracle_and_join(oracle, case):
+    """gsj_bruteforce_count (the reference's GPU algorithm 1) gives the oracle's
+    brute-force counts exactly, and the grid join's counts on these inputs."""
+    n, dt, N, eps = case
+    rng = np.random.default_rng(40 + n)
+    pts = (rng.uniform(0, 10, size=(N, n)) * rng.uniform(0.5, 2.0, n)).astype(dt)
+    with SelfJoin(0) as sj:
+        bc, bt = sj.bruteforce(pts, eps)
+    oc, ot = oracle.bruteforce_counts(pts, eps, oracle_cfg(oracle, min(6, n)))
+    assert bt == ot and np.array_equal(bc, oc)
+    gc, _, st = run_gpu(pts, eps, indexed_dims=min(6, n))
+    assert np.array_equal(gc, bc) and st["total_pairs"] == bt
+
+
 def test_deterministic_without_stamp():
     pts = synth.generate("c1_uniform2d")
     c1, t1, _ = run_gpu(pts, 1.0, indexed_dims=2)
