@@ -188,6 +188,90 @@ def _cpu_baseline(pts: np.ndarray, w, budget_s: float = 15.0) -> dict:
                       f"({sq:.2f} s); pairs/s extrapolated to all {N} queries"}
 
 
+# ------------------------------------------------------------------ request stream
+def _calibrate_eps(x, target: float, seed: int) -> float:
+    """eps with `target` mean neighbours per point (self included) on 256
+    seeded queries: the (256 * target)-th smallest of their squared distances
+    to all points (float64 on the device), i.e. the sample mean count at eps
+    is the target."""
+    import torch
+
+    N = x.shape[0]
+    g = torch.Generator(device=x.device)
+    g.manual_seed(seed)
+    q = x[torch.randperm(N, generator=g, device=x.device)[:256]].double()
+    qn = (q * q).sum(1, keepdim=True)
+    k = max(1, int(round(q.shape[0] * target)))
+    best = None
+    for c0 in range(0, N, 65536):
+        p = x[c0:c0 + 65536].double()
+        d2 = (qn + (p * p).sum(1)[None, :] - 2.0 * (q @ p.T)).clamp_min(0.0).reshape(-1)
+        cand = d2 if best is None else torch.cat([best, d2])
+        best = torch.topk(cand, min(k, cand.numel()), largest=False).values
+    return float(best.max().sqrt().item())
+
+
+def _requests(args) -> None:
+    """The 90-D workload's second phase: a seeded stream of independent joins
+    (N log-uniform in [10k, 500k], n from {8, 16, 32, 90}, eps for 10-100 mean
+    neighbours, the 90-D workload's switches), each through gsj_join on
+    device-resident points.  Reports the per-request latency (host wall clock
+    around the call, which returns when the join is done) and the stream's
+    result pairs per second."""
+    import time
+
+    import torch
+
+    from gpu_self_join_b200 import JoinConfig, SelfJoin, synth
+
+    rank, local_rank, world = _env_rank()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    reqs = synth.request_stream(args.requests)
+    prepared = []
+    for r in reqs:
+        x = torch.from_numpy(synth.gen_heavy(r.N, r.n, r.seed)).cuda()
+        prepared.append((r, x, _calibrate_eps(x, r.target_mean, r.seed)))
+    torch.cuda.synchronize()
+    sj = SelfJoin(local_rank)
+
+    def cfg_of(r):
+        return JoinConfig(indexed_dims=min(6, r.n), reorder=True, shortcircuit=True, ilp=8, stamp=False,
+                          query_reorder=True, plain=args.plain)
+
+    for r, x, eps in prepared[:max(3, args.warmup)]:
+        sj.run(x, eps, cfg_of(r))
+    torch.cuda.synchronize()
+    lat, pairs, paths = [], 0, {}
+    t_all = time.perf_counter()
+    for r, x, eps in prepared:
+        t0 = time.perf_counter()
+        st = sj.run(x, eps, cfg_of(r))
+        lat.append((time.perf_counter() - t0) * 1e3)
+        pairs += int(st["total_pairs"])
+        paths[int(st["join_path"])] = paths.get(int(st["join_path"]), 0) + 1
+    t_all = time.perf_counter() - t_all
+    sj.close()
+    lat_sorted = sorted(lat)
+
+    def pct(p):
+        return lat_sorted[min(len(lat_sorted) - 1, int(round(p / 100.0 * (len(lat_sorted) - 1))))]
+
+    line = {
+        "metric": "request stream: result pairs/s (256 joins, 90-D workload phase 2)", "value": pairs / t_all,
+        "unit": "pairs/s", "n_gpus": 1, "steps": len(prepared), "warmup": max(3, args.warmup),
+        "ms_per_step": t_all * 1e3 / len(prepared), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded request stream)",
+        "config": {"workload": "c5_requests", "requests": len(prepared), "plain": bool(args.plain),
+                   "N_range": [min(r.N for r, _, _ in prepared), max(r.N for r, _, _ in prepared)],
+                   "dims": sorted({r.n for r, _, _ in prepared}), "result_pairs": pairs,
+                   "join_paths": {str(k): v for k, v in sorted(paths.items())}},
+        "latency_ms": {"p50": pct(50), "p90": pct(90), "p99": pct(99), "max": lat_sorted[-1]},
+    }
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ our arm
 def _ours(args) -> None:
     import torch
@@ -367,11 +451,14 @@ def main():
                     help="generate a smaller instance of the workload (profiling captures only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--requests", type=int, default=256, help="joins in the c5_requests stream")
     ap.add_argument("--plain", action="store_true",
                     help="no tensor-core screen on high-dimensional workloads (exact FP32 for every pair)")
     args = ap.parse_args()
     if args.impl == "reference":
         _reference_arm(args)
+    elif args.workload == "c5_requests":
+        _requests(args)
     else:
         _ours(args)
 

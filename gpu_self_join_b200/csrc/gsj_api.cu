@@ -344,7 +344,7 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         double* partial = nullptr;
         GSJ_TRY(dev_get(c, c->srows, N * (sc.kpad / 8), &rows));
         GSJ_TRY(dev_get(c, c->snorms, N, &norms));
-        GSJ_TRY(dev_get(c, c->spartial, (size_t)kScreenPrepBlocks * a.n, &partial));
+        GSJ_TRY(dev_get(c, c->spartial, (size_t)kScreenPrepBlocks * a.n * 2, &partial));
         GSJ_TRY(dev_get(c, c->scentre, a.n, &centre));
         S.kernel_launches += 3;
         GSJ_CUDA(c, launch_screen_prep(a.pts, (uint32_t)N, a.n, a.npad, sc.kpad, partial, centre, rows, norms, st));

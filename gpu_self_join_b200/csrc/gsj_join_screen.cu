@@ -719,24 +719,37 @@ cudaError_t launch_recheck_one(const JoinArgs<float>& a, const unsigned long lon
     return cudaGetLastError();
 }
 
-// Per-block FP64 column sums over a fixed row range (deterministic).
+// Per-block FP64 column sums and counts of the finite values over a fixed row
+// range (deterministic).  Non-finite coordinates are left out of the centre,
+// so that only their own rows (and pairs) become inconclusive for the screen.
 __global__ void k_col_partial(const float* __restrict__ pts, uint32_t N, uint32_t n, uint32_t npad,
                               double* __restrict__ partial) {
     const uint32_t per = (N + gridDim.x - 1) / gridDim.x;
     const uint32_t r0 = blockIdx.x * per, r1 = min(N, r0 + per);
     for (uint32_t d = threadIdx.x; d < n; d += blockDim.x) {
-        double acc = 0.0;
-        for (uint32_t r = r0; r < r1; r++) acc += (double)pts[(size_t)r * npad + d];
-        partial[(size_t)blockIdx.x * n + d] = acc;
+        double acc = 0.0, cnt = 0.0;
+        for (uint32_t r = r0; r < r1; r++) {
+            const float v = pts[(size_t)r * npad + d];
+            if (isfinite(v)) {
+                acc += (double)v;
+                cnt += 1.0;
+            }
+        }
+        partial[((size_t)blockIdx.x * n + d) * 2] = acc;
+        partial[((size_t)blockIdx.x * n + d) * 2 + 1] = cnt;
     }
 }
 
-__global__ void k_col_mean(const double* __restrict__ partial, uint32_t nblocks, uint32_t N, uint32_t n,
+__global__ void k_col_mean(const double* __restrict__ partial, uint32_t nblocks, uint32_t n,
                            float* __restrict__ centre) {
     for (uint32_t d = threadIdx.x; d < n; d += blockDim.x) {
-        double acc = 0.0;
-        for (uint32_t b = 0; b < nblocks; b++) acc += partial[(size_t)b * n + d];
-        centre[d] = N ? (float)(acc / (double)N) : 0.f;
+        double acc = 0.0, cnt = 0.0;
+        for (uint32_t b = 0; b < nblocks; b++) {
+            acc += partial[((size_t)b * n + d) * 2];
+            cnt += partial[((size_t)b * n + d) * 2 + 1];
+        }
+        const double m = cnt > 0.0 ? acc / cnt : 0.0;
+        centre[d] = isfinite(m) ? (float)m : 0.f;
     }
 }
 
@@ -778,7 +791,7 @@ cudaError_t launch_screen_prep(const float* pts, uint32_t N, uint32_t n, uint32_
     if (N == 0) return cudaSuccess;
     if (kpad < n + 2u || (kpad & 7u)) return cudaErrorInvalidValue;
     k_col_partial<<<kScreenPrepBlocks, 128, 0, st>>>(pts, N, n, npad, partial);
-    k_col_mean<<<1, 128, 0, st>>>(partial, kScreenPrepBlocks, N, n, centre);
+    k_col_mean<<<1, 128, 0, st>>>(partial, kScreenPrepBlocks, n, centre);
     uint64_t blocks = ((uint64_t)N + 255) / 256;
     if (blocks > 148u * 16u) blocks = 148u * 16u;
     k_screen_rows<<<(unsigned)blocks, 256, 0, st>>>(pts, N, n, npad, kpad, centre, rows, norms);

@@ -118,8 +118,8 @@ struct ScreenConst {
     const float* norms;   // [N] |c^|^2 (FP32 sum of the BF16 squares)
 };
 // Centred BF16 rows and norms of all points (slot order) for the screen:
-// centre = per-dimension mean (deterministic two-level FP64 sum); `partial`
-// holds kScreenPrepBlocks x n doubles, `centre` n floats.
+// centre = per-dimension mean of the finite values (deterministic two-level
+// FP64 sum); `partial` holds kScreenPrepBlocks x n x 2 doubles, `centre` n floats.
 constexpr uint32_t kScreenPrepBlocks = 256;
 cudaError_t launch_screen_prep(const float* pts, uint32_t N, uint32_t n, uint32_t npad, uint32_t kpad,
                                double* partial, float* centre, uint4* rows, float* norms, cudaStream_t st);

@@ -123,6 +123,49 @@ def gen_c5(N: int = 515_345) -> np.ndarray:
     return np.concatenate([g, t], axis=1).astype(np.float32)
 
 
+def gen_heavy(N: int, n: int, seed: int) -> np.ndarray:
+    """The 90-D workload's distribution at another dimensionality: the first
+    min(12, n) dims Gaussian with variances log-U[1,100], the rest
+    multivariate Student-t (nu = 3) with a low-rank (<= 8) factor correlation
+    plus diagonal."""
+    rng = np.random.default_rng(seed)
+    ng = min(12, n)
+    var = np.exp(rng.uniform(np.log(1.0), np.log(100.0), size=ng))
+    g = rng.standard_normal((N, ng)) * np.sqrt(var)
+    m = n - ng
+    if m == 0:
+        return g.astype(np.float32)
+    r = min(8, m)
+    F = rng.standard_normal((m, r)) * 0.6
+    diag = rng.uniform(0.3, 1.0, size=m)
+    z = rng.standard_normal((N, r)) @ F.T + rng.standard_normal((N, m)) * np.sqrt(diag)
+    chi = rng.chisquare(3.0, size=(N, 1))
+    return np.concatenate([g, z / np.sqrt(chi / 3.0)], axis=1).astype(np.float32)
+
+
+@dataclass(frozen=True)
+class Request:
+    index: int
+    N: int
+    n: int
+    target_mean: float  # mean neighbours per point the request's eps is chosen for
+    seed: int
+
+
+def request_stream(count: int = 256) -> list[Request]:
+    """The 90-D workload's second phase: `count` independent self-joins, N
+    log-uniform in [10k, 500k], n from {8, 16, 32, 90}, a target of 10-100
+    mean neighbours each (seed BASE_SEED + 5)."""
+    rng = np.random.default_rng(BASE_SEED + 5)
+    out = []
+    for i in range(count):
+        N = int(round(np.exp(rng.uniform(np.log(10_000), np.log(500_000)))))
+        n = int(rng.choice([8, 16, 32, 90]))
+        target = float(rng.uniform(10.0, 100.0))
+        out.append(Request(i, N, n, target, int(rng.integers(0, 2**31 - 1))))
+    return out
+
+
 GENERATORS = {"c1_uniform2d": gen_c1, "c2_gmm2d": gen_c2, "c3_gmm6d": gen_c3, "c4_derived18d": gen_c4,
               "c5_heavy90d": gen_c5}
 

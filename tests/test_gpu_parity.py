@@ -141,6 +141,21 @@ def test_tile_join_matches_oracle(oracle, case, plain):
         assert st["screen_rechecks"] < st["candidates"]
 
 
+@pytest.mark.parametrize("stamp", [False, True])
+def test_screen_with_nonfinite_points(oracle, stamp):
+    """A NaN and an infinite coordinate in non-indexed dimensions (the six
+    indexed ones are the high-variance dims 0-5; rows 5 and 17 are outside
+    REORDER's every-100th sample): those points have no neighbours, not even
+    themselves, in the reference's arithmetic; every other list is unchanged,
+    and the screen still rejects the bulk of the candidates."""
+    pts = tile_points(18, 20000, 3.0, 77)
+    pts[5, 8] = np.nan
+    pts[17, 12] = np.inf
+    st = assert_same(oracle, pts, 3.0, indexed_dims=6, reorder=True, ilp=8, shortcircuit=True, stamp=stamp)
+    assert st["join_path"] == 3
+    assert st["screen_rechecks"] < st["candidates"] // 4
+
+
 def test_tile_join_deterministic():
     pts = tile_points(18, 20000, 3.0, 7)
     c1, t1, s1 = run_gpu(pts, 3.0, indexed_dims=6, stamp=True)
