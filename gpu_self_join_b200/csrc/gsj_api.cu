@@ -143,7 +143,7 @@ struct gsj_context {
     Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
         item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
-        minmax_part, pairs, pairs2, srows, snorms, spartial, scentre, unc, table2;
+        minmax_part, pairs, pairs2, srows, snorms, spartial, scentre, unc, table2, nbtab;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
     // last result
@@ -304,6 +304,121 @@ int validate(gsj_context* c, const gsj_config& cfg, uint64_t N) {
     return GSJ_OK;
 }
 
+// ------------------------------------------------------------------ pair keys -> table
+// Sorts `nsort` packed (query id << shift | candidate id) keys on the device
+// (entries past the R real keys are pads, which sort last), writes the
+// neighbour table (low bits) and the list lengths and offsets, and fills the
+// stage times and the result state.  cand: the device candidate counter.
+int pairs_to_csr(gsj_context* c, unsigned long long* pairs, uint64_t nsort, uint64_t R, uint32_t shift, uint64_t N,
+                 uint32_t* counts, uint64_t* offsets, const unsigned long long* cand) {
+    gsj_stats& S = c->stats;
+    cudaStream_t st = c->st;
+    GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
+    unsigned long long* sorted = nullptr;
+    uint32_t* table = nullptr;
+    GSJ_TRY(dev_get(c, c->pairs2, nsort ? nsort : 1, &sorted));
+    GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
+    GSJ_CUDA(c, cudaMemsetAsync(counts, 0, (N + 1) * sizeof(uint32_t), st));
+    if (R) {
+        // one bit above the keys, clear in every key and set in the pads
+        const int end_bit = (int)(2 * shift + 1);
+        size_t tb = 0;
+        void* temp = nullptr;
+        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, tb, pairs, sorted, (uint64_t)nsort, 0, end_bit, st));
+        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
+        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(temp, tb, pairs, sorted, (uint64_t)nsort, 0, end_bit, st));
+        S.kernel_launches += (uint64_t)(end_bit + 7) / 8 + 2;
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_pairs_to_table(sorted, R, shift, table, counts, c->num_sms, st));
+    }
+    void* stemp = nullptr;
+    GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
+    S.kernel_launches += 3;
+    GSJ_CUDA(c, scan_u32_u64(counts, offsets, N, stemp, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
+    uint64_t total = 0;
+    GSJ_TRY(d2h_small(c, &total, offsets + N, 1));
+    if (total != R) return fail(c, GSJ_ERR_STATE, "list lengths disagree with the pair count");
+    unsigned long long ncand = 0;
+    GSJ_TRY(d2h_small(c, &ncand, cand, 1));
+    {
+        float ms = 0;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
+        S.dev_ms_index = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[2], c->tev[3]));
+        S.dev_ms_count = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[4], c->tev[5]));
+        S.dev_ms_fill = ms;
+    }
+    S.candidates = ncand;
+    S.total_pairs = R;
+    c->R = R;
+    c->have_result = true;
+    return GSJ_OK;
+}
+
+// ------------------------------------------------------------------ warp join (emit)
+// The warp-per-item traversal in one pass: k_join's pass kEmit appends every
+// pair as a packed key (sampling pass over every kSampleStride-th item to size
+// the buffer; a short buffer is re-sized exactly and the pass repeated), then
+// the keys are sorted into the table.
+template <typename T>
+int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model, bool rows, uint32_t* counts,
+              uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
+    constexpr uint32_t kSampleStride = 64;
+    gsj_stats& S = c->stats;
+    cudaStream_t st = c->st;
+    uint32_t shift = 1;
+    while (shift < 32 && ((N - 1) >> shift)) shift++;
+    const uint32_t ni = a.num_items;
+    TileOut o{};
+    o.cursor = cursor;       // entries reserved (blocks)
+    o.rechecks = cursor + 1; // keys emitted (exact)
+    o.shift = shift;
+    unsigned long long* cand = reinterpret_cast<unsigned long long*>(a.work_counter + 2);
+    // entries the warps may leave unused at the end: one block per resident warp
+    const uint64_t slack = (uint64_t)c->num_sms * 64u * kScreenBlockSlack;
+    auto reset = [&]() -> int {
+        GSJ_CUDA(c, cudaMemsetAsync(a.work_counter, 0, 4 * sizeof(uint32_t), st));
+        GSJ_CUDA(c, cudaMemsetAsync(cursor, 0, 2 * sizeof(unsigned long long), st));
+        return GSJ_OK;
+    };
+    GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
+    const uint32_t nsample = (ni + kSampleStride - 1) / kSampleStride;
+    GSJ_TRY(reset());
+    o.emit = false;
+    o.stride = kSampleStride;
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_join<T>(a, kEmit, model, stamp, rows, c->num_sms, st, &o, nsample));
+    unsigned long long sampled = 0;
+    GSJ_TRY(d2h_small(c, &sampled, o.rechecks, 1));
+    const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
+    uint64_t cap = (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
+    unsigned long long* pairs = nullptr;
+    unsigned long long used = 0, R = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        GSJ_TRY(dev_get(c, c->pairs, cap, &pairs));
+        GSJ_TRY(reset());
+        o.emit = true;
+        o.stride = 1;
+        o.pairs = pairs;
+        o.cap = cap;
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_join<T>(a, kEmit, model, stamp, rows, c->num_sms, st, &o, ni));
+        GSJ_TRY(d2h_small(c, &used, cursor, 1));
+        GSJ_TRY(d2h_small(c, &R, o.rechecks, 1));
+        if (used <= cap) break;
+        if (attempt == 1) return fail(c, GSJ_ERR_STATE, "warp join: pair count changed between two passes");
+        cap = R + slack;
+    }
+    GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
+    GSJ_TRY(pairs_to_csr(c, pairs, used, R, shift, N, counts, offsets, cand));
+    S.join_path = GSJ_PATH_WARP;
+    S.ms_join = now_ms() - t_join;
+    S.ms_total = now_ms() - t_start;
+    return GSJ_OK;
+}
+
 // ------------------------------------------------------------------ tile join
 // Count, pair buffer, sort and table of the tile join (high-dimensional float
 // data).  A sampling pass over every kSampleStride-th item sizes the pair
@@ -411,49 +526,10 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         R = U;
     }
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
-    // ---- on-device pair sort -> neighbour table in point-id order
-    GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
-    unsigned long long* sorted = nullptr;
-    uint32_t* table = nullptr;
-    GSJ_TRY(dev_get(c, c->pairs2, R ? R : 1, &sorted));
-    GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
-    GSJ_CUDA(c, cudaMemsetAsync(counts, 0, (N + 1) * sizeof(uint32_t), st));
-    if (R) {
-        size_t tb = 0;
-        void* temp = nullptr;
-        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, tb, pairs, sorted, (uint64_t)R, 0, (int)(2 * shift), st));
-        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(temp, tb, pairs, sorted, (uint64_t)R, 0, (int)(2 * shift), st));
-        S.kernel_launches += 2 * shift / 8 + 2;
-        S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_pairs_to_table(sorted, R, shift, table, counts, c->num_sms, st));
-    }
-    void* stemp = nullptr;
-    GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
-    S.kernel_launches += 3;
-    GSJ_CUDA(c, scan_u32_u64(counts, offsets, N, stemp, st));
-    GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
-    uint64_t total = 0;
-    GSJ_TRY(d2h_small(c, &total, offsets + N, 1));
-    if (total != R) return fail(c, GSJ_ERR_STATE, "tile join: list lengths disagree with the pair count");
-    unsigned long long ncand = 0;
-    GSJ_TRY(d2h_small(c, &ncand, cand, 1));
-    {
-        float ms = 0;
-        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
-        S.dev_ms_index = ms;
-        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[2], c->tev[3]));
-        S.dev_ms_count = ms;
-        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[4], c->tev[5]));
-        S.dev_ms_fill = ms;
-    }
-    S.candidates = ncand;
+    GSJ_TRY(pairs_to_csr(c, pairs, R, R, shift, N, counts, offsets, cand));
     S.screen_rechecks = screen ? U : 0;
     S.join_path = screen ? GSJ_PATH_SCREEN : GSJ_PATH_TILE;
     S.ms_join = now_ms() - t_join;
-    S.total_pairs = R;
-    c->R = R;
-    c->have_result = true;
     S.ms_total = now_ms() - t_start;
     return GSJ_OK;
 }
@@ -559,6 +635,30 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         totalCells = (j == 0) ? g.ncells[0] : totalCells * g.ncells[j];
     }
     S.total_cells = totalCells;
+    // neighbour offsets in the kernels' order (digit j of o is dim j's step + 1):
+    // linear-id delta, moved-down / moved-up dims, highest moved dim
+    uint4* d_nbtab = nullptr;
+    {
+        uint32_t noff = 1;
+        for (uint32_t j = 0; j < k; j++) noff *= 3u;
+        std::vector<uint4> tab(noff);
+        for (uint32_t o = 0; o < noff; o++) {
+            long long delta = 0;
+            uint32_t down = 0, up = 0, hd = 0xffu, t = o;
+            for (uint32_t j = 0; j < k; j++) {
+                const int dl = (int)(t % 3u) - 1;
+                t /= 3u;
+                delta += (long long)dl * (long long)g.mult[j];
+                if (dl < 0) down |= 1u << j;
+                if (dl > 0) up |= 1u << j;
+                if (dl != 0) hd = j;
+            }
+            const uint64_t d = (uint64_t)delta;
+            tab[o] = make_uint4((uint32_t)d, (uint32_t)(d >> 32), down | (up << 16), hd);
+        }
+        GSJ_TRY(dev_get(c, c->nbtab, noff, &d_nbtab));
+        GSJ_CUDA(c, cudaMemcpyAsync(d_nbtab, tab.data(), noff * sizeof(uint4), cudaMemcpyHostToDevice, st));
+    }
     T* d_min = nullptr;
     GSJ_TRY(dev_get(c, c->minarr, k, &d_min));
     GSJ_CUDA(c, cudaMemcpyAsync(d_min, minArr.data(), k * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -728,6 +828,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.hmask = hmask;
     a.items = items;
     a.num_items = num_items;
+    a.nbtab = d_nbtab;
     a.work_counter = ctr;
     a.n = n;
     a.npad = npad;
@@ -746,6 +847,11 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
             unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
             return tile_join(c, a, N, stamp, model, screen, counts, offsets, cursor, t_join, t_start);
         }
+    }
+    // Every other grid except the thread-per-query rows: one emit pass + pair sort.
+    if (!tpq) {
+        unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
+        return emit_join<T>(c, a, N, stamp, model, rows, counts, offsets, cursor, t_join, t_start);
     }
     // On the row-range path the distance work is cheap, so the fill pass walks
     // the full neighbourhood and writes every list forward only (contiguous,
@@ -918,7 +1024,7 @@ int gsj_destroy(gsj_context* c) {
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
                    &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
                    &c->minarr,   &c->minmax_part, &c->pairs, &c->pairs2, &c->srows, &c->snorms,
-                   &c->spartial, &c->scentre, &c->unc, &c->table2};
+                   &c->spartial, &c->scentre, &c->unc, &c->table2, &c->nbtab};
     for (Buf* b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})

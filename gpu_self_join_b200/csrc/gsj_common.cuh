@@ -18,7 +18,7 @@ constexpr uint64_t kEmptyKey = ~0ull;        // hash table empty slot
 //   kIlpSc  ILP>0,  SHORTCIRCUIT=1  per ILP block: s = fma(d_l, d_l, s); s += d_{l+j}^2 (j >= 1)
 enum Model : int { kSeq = 0, kIlp = 1, kIlpSc = 2 };
 
-enum Pass : int { kCount = 0, kFill = 1 };
+enum Pass : int { kCount = 0, kFill = 1, kEmit = 2 };
 
 // Grid geometry (k <= kMaxK indexed dims).
 struct GridGeom {
@@ -40,6 +40,8 @@ struct JoinArgs {
     const uint32_t* hvals;        // [hcap] cell indices
     uint64_t hmask;               // hcap - 1
     const uint2* items;           // [num_items] (cell, chunk)
+    const uint4* nbtab;           // [3^k] neighbour offsets: linear-id delta (x lo, y hi), z = moved-down dims
+                                  // | moved-up dims << 16, w = highest moved dim (0xff: none)
     uint32_t num_items;
     uint32_t* work_counter;       // dynamic work distribution
     uint32_t n, npad, ilp;
@@ -68,6 +70,35 @@ __host__ __device__ inline uint64_t mix64(uint64_t x) {
     x *= 0x94d049bb133111ebull;
     x ^= x >> 31;
     return x;
+}
+
+// Neighbour offset `o` of a cell: usable when it stays inside the grid (no
+// moved-down dim at the cell's low edge, no moved-up dim at its high edge) and,
+// with unicomp, when the highest moved dim has an odd own coordinate
+// (stamploops.h: `nDCellIDs[d] & 1`; the cell itself is always visited).
+// Returns the neighbour's linear id in `lin`.
+template <typename T, bool STAMP>
+__device__ __forceinline__ bool nb_offset(const JoinArgs<T>& a, uint32_t o, uint64_t own_lin, uint32_t lowmask,
+                                          uint32_t highmask, uint32_t oddmask, uint64_t& lin) {
+    const uint4 e = a.nbtab[o];
+    if ((e.z & 0xffffu) & lowmask) return false;
+    if ((e.z >> 16) & highmask) return false;
+    if (STAMP && e.w != 0xffu && !((oddmask >> e.w) & 1u)) return false;
+    lin = own_lin + (((uint64_t)e.y << 32) | e.x);
+    return true;
+}
+
+// Edge and parity masks of a cell's coordinates for nb_offset.
+__device__ __forceinline__ void cell_masks(const uint32_t (&own)[kMaxK], const GridGeom& g, uint32_t& lowmask,
+                                           uint32_t& highmask, uint32_t& oddmask) {
+    lowmask = highmask = oddmask = 0u;
+#pragma unroll
+    for (int j = 0; j < kMaxK; j++)
+        if (j < (int)g.k) {
+            lowmask |= (own[j] == 0u ? 1u : 0u) << j;
+            highmask |= (own[j] + 1u >= g.ncells[j] ? 1u : 0u) << j;
+            oddmask |= (own[j] & 1u) << j;
+        }
 }
 
 // Slot range of the cell with linear id `lin`: from the dense slot-prefix

@@ -19,8 +19,9 @@ namespace gsj {
 // ------------------------------------------------------------ REORDER statistic
 // One block.  Thread i owns dimension i and adds the sampled values in the
 // reference's sequential order (rows 0, 100, 200, ...), unfused, in T.  The
-// sampled rows are staged through shared memory in chunks so that the
-// sequential chains run on on-chip data.
+// sampled rows are staged through shared memory in chunks by the whole block
+// (up to 1024 threads, many loads in flight) so that the sequential chains run
+// on on-chip data.
 template <typename T>
 __global__ void k_variance(const T* __restrict__ in, uint64_t N, uint32_t n, T denom,
                            T* __restrict__ var_out) {
@@ -270,7 +271,10 @@ static inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n
 
 template <typename T>
 cudaError_t launch_variance(const T* in, uint64_t N, uint32_t n, T denom, T* var_out, cudaStream_t st) {
-    const unsigned threads = n < 32 ? 32 : (n > 1024 ? 1024 : ((n + 31) / 32) * 32);
+    // the staging uses every thread; the sums use the first n (d0 loop above 1024)
+    const unsigned threads = 1024;
+    cudaError_t e = cudaFuncSetAttribute(k_variance<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kVarStageBytes);
+    if (e != cudaSuccess) return e;
     k_variance<T><<<1, threads, kVarStageBytes, st>>>(in, N, n, denom, var_out);
     return cudaGetLastError();
 }

@@ -65,9 +65,39 @@ __host__ __device__ inline WarpSmem warp_smem_layout(uint32_t npad, uint32_t tsi
     return w;
 }
 
+// Pass kEmit: the warp appends its hits as packed (query id << shift |
+// candidate id) keys, and with unicomp the reverse key of a hit in another
+// cell, into blocks of kEmitBlk entries it reserves on o.cursor (unused tails
+// padded with kUndecidedPad, which sorts after every key); emitted counts the
+// keys exactly.  hit / cr are this lane's flags, b / cb their ballots.
+constexpr uint32_t kEmitBlk = (uint32_t)kScreenBlockSlack;
+
+__device__ __forceinline__ void emit_keys(const TileOut& o, unsigned long long& blk_base, uint32_t& blk_used,
+                                          unsigned long long& emitted, bool hit, bool cr, unsigned b, unsigned cb,
+                                          unsigned lt, int lane, uint64_t qid, uint64_t cid) {
+    const uint32_t cnt = (uint32_t)__popc(b) + (uint32_t)__popc(cb);
+    emitted += cnt;
+    if (!o.emit) return;
+    if (blk_used + cnt > kEmitBlk) {
+        for (uint32_t e = blk_used + (uint32_t)lane; e < kEmitBlk; e += 32u)
+            if (blk_base + e < o.cap) o.pairs[blk_base + e] = kUndecidedPad;
+        unsigned long long nb = 0;
+        if (lane == 0) nb = atomicAdd(o.cursor, (unsigned long long)kEmitBlk);
+        blk_base = __shfl_sync(0xffffffffu, nb, 0);
+        blk_used = 0;
+    }
+    if (hit) {
+        unsigned long long p = blk_base + blk_used + (unsigned)__popc(b & lt) + (unsigned)__popc(cb & lt);
+        if (p < o.cap) o.pairs[p] = (qid << o.shift) | cid;
+        p++;
+        if (cr && p < o.cap) o.pairs[p] = (cid << o.shift) | qid;
+    }
+    blk_used += cnt;
+}
+
 template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS, bool ROWS>
 __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff,
-                                              uint32_t batch) {
+                                              uint32_t batch, const TileOut o, uint32_t nvisit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool GENERIC = (NT == 0);
     const unsigned FULL = 0xffffffffu;
@@ -84,19 +114,22 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
     const unsigned lt = lanemask_lt();
     const uint32_t k = a.g.k;
     unsigned long long cand_total = 0;
+    unsigned long long blk_base = 0, emitted = 0;  // pass kEmit
+    uint32_t blk_used = kEmitBlk;
 
-    // work items are claimed `batch` at a time (one atomic per batch)
+    // work items are claimed `batch` at a time (one atomic per batch); item i
+    // is items[i * o.stride] (a stride above 1 samples every stride-th item)
     uint32_t item = 0, item_end = 0;
     for (;;) {
         if (item >= item_end) {
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(a.work_counter, batch);
             base = __shfl_sync(FULL, base, 0);
-            if (base >= a.num_items) break;
+            if (base >= nvisit) break;
             item = base;
-            item_end = min(base + batch, a.num_items);
+            item_end = min(base + batch, nvisit);
         }
-        const uint2 wi = a.items[item++];
+        const uint2 wi = a.items[(size_t)(item++) * o.stride];
         const uint32_t cell = wi.x;
         const uint32_t cs = a.cell_start[cell], ce = a.cell_start[cell + 1];
         const uint32_t q0 = cs + wi.y * kQChunk;
@@ -141,29 +174,13 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                                                                        a.eps))
                                       : 0u;
             // ---- neighbour cells (kernel.cu:180-303; stamploops.h for STAMP)
+            uint32_t lowmask, highmask, oddmask;
+            cell_masks(own, a.g, lowmask, highmask, oddmask);
+            const uint64_t own_lin = a.cell_key[cell];
             for (uint32_t base = 0; base < noff; base += 32) {
                 const uint32_t o = base + lane;
-                bool ok = o < noff;
                 uint64_t lin = 0;
-                bool moved = false, hd_odd = false;
-                uint32_t t = o;
-#pragma unroll
-                for (int j = 0; j < kMaxK; j++) {
-                    if (j < (int)k) {
-                        const int dl = (int)(t % 3u) - 1;
-                        t /= 3u;
-                        const long long nbj = (long long)own[j] + dl;
-                        if (nbj < 0 || nbj >= (long long)a.g.ncells[j]) ok = false;
-                        lin += (uint64_t)nbj * a.g.mult[j];
-                        if (dl != 0) {
-                            moved = true;
-                            hd_odd = (own[j] & 1u) != 0;  // highest differing dim wins
-                        }
-                    }
-                }
-                // unicomp: a neighbour whose highest differing dim d has an even own
-                // coordinate is visited from the other cell (stamploops.h: `nDCellIDs[d] & 1`)
-                if (STAMP && moved && !hd_odd) ok = false;
+                const bool ok = o < noff && nb_offset<T, STAMP>(a, o, own_lin, lowmask, highmask, oddmask, lin);
                 uint32_t st = 0, cnt = 0;
                 const bool found = ok && lookup_range(a, lin, st, cnt);
                 const unsigned m = __ballot_sync(FULL, found);
@@ -197,10 +214,11 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
         for (uint32_t e = lane; e < qn * npad; e += 32) q_s[e] = a.pts[(size_t)q0 * npad + e];
         if (lane < qn) qid_s[lane] = a.ids[q0 + lane];
         __syncwarp();
-        if (PASS == kCount) cand_total += (unsigned long long)total * qn;
+        if (PASS != kFill) cand_total += (unsigned long long)total * qn;
         uint32_t myq = 0;                 // count pass: lane j holds query j's forward count
         unsigned long long mycur = 0;     // fill pass: lane j holds query j's next table position
         if (PASS == kFill && lane < qn) mycur = a.offsets[qid_s[lane]];
+        const uint64_t my_qid = lane < qn ? qid_s[lane] : 0u;  // pass kEmit
 
         if constexpr (!GENERIC) {
             // ---- register path (n <= 8): up to G tiles of 32 candidates live in
@@ -229,7 +247,7 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                     }
                     cslot[t] = slot;
                     ccross[t] = STAMP && cval[t] && (slot < cs || slot >= ce);
-                    cid[t] = (PASS == kFill && cval[t]) ? a.ids[slot] : 0u;
+                    cid[t] = (PASS != kCount && cval[t]) ? a.ids[slot] : 0u;
                     const T* row = a.pts + (size_t)slot * npad;
 #pragma unroll
                     for (int l = 0; l < NR; l++) cx[t][l] = row[l];
@@ -253,7 +271,7 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                             if (PASS == kCount) {
                                 cntj += __popc(b);
                                 if (STAMP && ccross[t] && hit) rev[t]++;
-                            } else {
+                            } else if (PASS == kFill) {
                                 if (hit) {
                                     const unsigned long long pos = cur + __popc(b & lt);
                                     if (pos < a.table_cap) a.table[pos] = cid[t];
@@ -261,12 +279,17 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                                 }
                                 cur += __popc(b);
                                 if (STAMP && ccross[t] && hit) revmask[t] |= 1u << j;
+                            } else if (b) {
+                                const bool cr = STAMP && ccross[t] && hit;
+                                const unsigned cb = __ballot_sync(FULL, cr);
+                                emit_keys(o, blk_base, blk_used, emitted, hit, cr, b, cb, lt, lane,
+                                          __shfl_sync(FULL, my_qid, j), cid[t]);
                             }
                         }
                     }
                     if (PASS == kCount) {
                         if (lane == (int)j) myq += cntj;
-                    } else {
+                    } else if (PASS == kFill) {
                         if (lane == (int)j) mycur = cur;
                     }
                 }
@@ -274,7 +297,7 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                 for (int t = 0; t < G; t++) {
                     if (PASS == kCount) {
                         if (STAMP && rev[t]) atomicAdd(&a.rev_cnt[cslot[t]], rev[t]);
-                    } else if (STAMP && revmask[t]) {
+                    } else if (PASS == kFill && STAMP && revmask[t]) {
                         unsigned long long pos =
                             atomicAdd(&a.rev_cursor[cslot[t]], (unsigned long long)__popc(revmask[t]));
                         uint32_t m = revmask[t];
@@ -318,6 +341,13 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                     if (PASS == kCount) {
                         if (lane == (int)j) myq += __popc(b);
                         if (STAMP && cross && hit) myrev++;
+                    } else if (PASS == kEmit) {
+                        if (b) {
+                            const bool cr = STAMP && cross && hit;
+                            const unsigned cb = __ballot_sync(FULL, cr);
+                            emit_keys(o, blk_base, blk_used, emitted, hit, cr, b, cb, lt, lane,
+                                      __shfl_sync(FULL, my_qid, j), corig);
+                        }
                     } else {
                         const unsigned long long cur = __shfl_sync(FULL, mycur, j);
                         if (hit) {
@@ -331,7 +361,7 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                 }
                 if (PASS == kCount) {
                     if (STAMP && myrev) atomicAdd(&a.rev_cnt[slot], myrev);
-                } else if (STAMP && revmask) {
+                } else if (PASS == kFill && STAMP && revmask) {
                     unsigned long long pos = atomicAdd(&a.rev_cursor[slot], (unsigned long long)__popc(revmask));
                     while (revmask) {
                         const int j = __ffs(revmask) - 1;
@@ -347,12 +377,19 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
         if (PASS == kCount && lane < qn) a.fwd_cnt[q0 + lane] = myq;
         __syncwarp();
     }
-    if (PASS == kCount && lane == 0 && cand_total) atomicAdd(a.cand_cnt, cand_total);
+    if (PASS != kFill && lane == 0 && cand_total && (PASS == kCount || o.emit)) atomicAdd(a.cand_cnt, cand_total);
+    if (PASS == kEmit) {
+        if (o.emit && blk_used < kEmitBlk)
+            for (uint32_t e = blk_used + (uint32_t)lane; e < kEmitBlk; e += 32u)
+                if (blk_base + e < o.cap) o.pairs[blk_base + e] = kUndecidedPad;
+        if (lane == 0 && emitted) atomicAdd(o.rechecks, emitted);
+    }
 }
 
 // ------------------------------------------------------------------ launch
 template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS, bool ROWS>
-static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, int num_sms, cudaStream_t st) {
+static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, const TileOut& o,
+                              uint32_t nvisit, int num_sms, cudaStream_t st) {
     auto kern = k_join<T, NT, MODEL, POL, STAMP, PASS, ROWS>;
     const WarpSmem L = warp_smem_layout(a.npad, sizeof(T), nb_cap, NT == 0);
     const uint32_t max_smem = 200u * 1024u;
@@ -371,69 +408,84 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     e = blocks_per_sm((const void*)kern, threads, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    const uint64_t needed = ((uint64_t)a.num_items + warps - 1) / warps;
+    const uint64_t needed = ((uint64_t)nvisit + warps - 1) / warps;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > needed) blocks = needed ? needed : 1;
     const uint64_t total_warps = blocks * (uint64_t)warps;
-    uint64_t batch = a.num_items / (total_warps * 16u);
+    uint64_t batch = nvisit / (total_warps * 16u);
     batch = batch < 1 ? 1 : (batch > 32 ? 32 : batch);
-    kern<<<(unsigned)blocks, threads, smem, st>>>(a, nb_cap, noff, (uint32_t)batch);
+    kern<<<(unsigned)blocks, threads, smem, st>>>(a, nb_cap, noff, (uint32_t)batch, o, nvisit);
     return cudaGetLastError();
 }
 
 template <typename T, int MODEL, int POL, bool STAMP, int PASS>
-static cudaError_t dispatch_nt(const JoinArgs<T>& a, bool rows, uint32_t nb_cap, uint32_t noff, int num_sms,
-                               cudaStream_t st) {
+static cudaError_t dispatch_nt(const JoinArgs<T>& a, bool rows, uint32_t nb_cap, uint32_t noff, const TileOut& o,
+                               uint32_t nvisit, int num_sms, cudaStream_t st) {
     if (rows) {
         // low-dimensional dense grids (k <= 3): registers for n <= 4
         if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
             switch (a.n) {
-                case 1: return launch_one<T, 1, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
-                case 2: return launch_one<T, 2, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
-                case 3: return launch_one<T, 3, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
-                case 4: return launch_one<T, 4, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
+                case 1: return launch_one<T, 1, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+                case 2: return launch_one<T, 2, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+                case 3: return launch_one<T, 3, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+                case 4: return launch_one<T, 4, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
                 default: break;
             }
         }
-        return launch_one<T, 0, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, num_sms, st);
+        return launch_one<T, 0, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
     }
     if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
         switch (a.n) {
-            case 6: return launch_one<T, 6, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, num_sms, st);
-            case 8: return launch_one<T, 8, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, num_sms, st);
+            case 6: return launch_one<T, 6, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
+            case 8: return launch_one<T, 8, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
             default: break;
         }
     }
-    return launch_one<T, 0, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, num_sms, st);
+    return launch_one<T, 0, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
 }
 
 template <typename T, bool STAMP, int PASS>
 static cudaError_t dispatch_model(const JoinArgs<T>& a, int model, bool rows, uint32_t nb_cap, uint32_t noff,
-                                  int num_sms, cudaStream_t st) {
+                                  const TileOut& o, uint32_t nvisit, int num_sms, cudaStream_t st) {
     constexpr int P = sizeof(T) == 8 ? kPolF64 : kPolF32;
     switch (model) {
-        case kSeq: return dispatch_nt<T, kSeq, P, STAMP, PASS>(a, rows, nb_cap, noff, num_sms, st);
-        case kIlp: return dispatch_nt<T, kIlp, P, STAMP, PASS>(a, rows, nb_cap, noff, num_sms, st);
-        case kIlpSc: return dispatch_nt<T, kIlpSc, P, STAMP, PASS>(a, rows, nb_cap, noff, num_sms, st);
+        case kSeq: return dispatch_nt<T, kSeq, P, STAMP, PASS>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
+        case kIlp: return dispatch_nt<T, kIlp, P, STAMP, PASS>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
+        case kIlpSc: return dispatch_nt<T, kIlpSc, P, STAMP, PASS>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <typename T>
 cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, bool rows, int num_sms,
-                        cudaStream_t st) {
+                        cudaStream_t st, const TileOut* emit, uint32_t nvisit) {
     uint32_t noff = 1;
     for (uint32_t j = 0; j < a.g.k; j++) noff *= 3u;
     if (rows && (a.g.k > 3 || !a.ds)) return cudaErrorInvalidValue;
     const uint32_t nb_cap = rows ? 32u : noff;
+    TileOut o{};
+    o.stride = 1;
+    if (pass == kEmit) {
+        if (!emit || emit->stride == 0) return cudaErrorInvalidValue;
+        o = *emit;
+    } else {
+        nvisit = a.num_items;
+    }
+    if (nvisit == 0) return cudaSuccess;
+    if ((uint64_t)(nvisit - 1) * o.stride >= a.num_items) return cudaErrorInvalidValue;
     if (pass == kCount)
-        return stamp ? dispatch_model<T, true, kCount>(a, model, rows, nb_cap, noff, num_sms, st)
-                     : dispatch_model<T, false, kCount>(a, model, rows, nb_cap, noff, num_sms, st);
-    return stamp ? dispatch_model<T, true, kFill>(a, model, rows, nb_cap, noff, num_sms, st)
-                 : dispatch_model<T, false, kFill>(a, model, rows, nb_cap, noff, num_sms, st);
+        return stamp ? dispatch_model<T, true, kCount>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st)
+                     : dispatch_model<T, false, kCount>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st);
+    if (pass == kEmit)
+        return stamp ? dispatch_model<T, true, kEmit>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st)
+                     : dispatch_model<T, false, kEmit>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st);
+    return stamp ? dispatch_model<T, true, kFill>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st)
+                 : dispatch_model<T, false, kFill>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st);
 }
 
-template cudaError_t launch_join<float>(const JoinArgs<float>&, int, int, bool, bool, int, cudaStream_t);
-template cudaError_t launch_join<double>(const JoinArgs<double>&, int, int, bool, bool, int, cudaStream_t);
+template cudaError_t launch_join<float>(const JoinArgs<float>&, int, int, bool, bool, int, cudaStream_t,
+                                        const TileOut*, uint32_t);
+template cudaError_t launch_join<double>(const JoinArgs<double>&, int, int, bool, bool, int, cudaStream_t,
+                                         const TileOut*, uint32_t);
 
 }  // namespace gsj

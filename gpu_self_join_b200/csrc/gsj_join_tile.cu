@@ -185,27 +185,13 @@ __global__ void __launch_bounds__(kThreads) k_tile_join(const JoinArgs<float> a,
                                   : 0u;
         // ---- neighbour cells in offset order (kernel.cu:180-303; stamploops.h)
         uint32_t nnb = 0;
+        uint32_t lowmask, highmask, oddmask;
+        cell_masks(own, a.g, lowmask, highmask, oddmask);
+        const uint64_t own_lin = a.cell_key[cell];
         for (uint32_t base = 0; base < noff; base += kThreads) {
             const uint32_t off = base + tid;
-            bool ok = off < noff;
             uint64_t lin = 0;
-            bool moved = false, hd_odd = false;
-            uint32_t t = off;
-#pragma unroll
-            for (int j = 0; j < kMaxK; j++) {
-                if (j < (int)k) {
-                    const int dl = (int)(t % 3u) - 1;
-                    t /= 3u;
-                    const long long nbj = (long long)own[j] + dl;
-                    if (nbj < 0 || nbj >= (long long)a.g.ncells[j]) ok = false;
-                    lin += (uint64_t)nbj * a.g.mult[j];
-                    if (dl != 0) {
-                        moved = true;
-                        hd_odd = (own[j] & 1u) != 0;  // highest differing dim wins
-                    }
-                }
-            }
-            if (STAMP && moved && !hd_odd) ok = false;
+            const bool ok = off < noff && nb_offset<float, STAMP>(a, off, own_lin, lowmask, highmask, oddmask, lin);
             uint32_t st = 0, cnt = 0;
             const bool found = ok && lookup_range(a, lin, st, cnt);
             const unsigned m = __ballot_sync(FULL, found);

@@ -37,7 +37,7 @@ inline cudaError_t blocks_per_sm(const void* kern, int threads, size_t smem, int
     return cudaSuccess;
 }
 
-constexpr unsigned kVarStageBytes = 32768;  // shared staging of sampled rows (REORDER statistic)
+constexpr unsigned kVarStageBytes = 98304;  // shared staging of sampled rows (REORDER statistic)
 
 template <typename T>
 cudaError_t launch_variance(const T* in, uint64_t N, uint32_t n, T denom, T* var_out, cudaStream_t st);
@@ -70,9 +70,13 @@ cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, cons
 // Join passes.  `pass` is kCount or kFill; `model` one of Model; `stamp`
 // selects the unicomp traversal.  The launcher picks the specialisation.
 // `rows` selects the dense low-dimensional specialisation (k <= 3, a.ds set).
+// Pass kEmit appends packed pair keys into *emit (TileOut; its rechecks
+// counter receives the exact number of keys) and visits items 0, stride, ...,
+// (nvisit - 1) * stride; the other passes visit every item.
+struct TileOut;
 template <typename T>
 cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, bool rows, int num_sms,
-                        cudaStream_t st);
+                        cudaStream_t st, const TileOut* emit = nullptr, uint32_t nvisit = 0);
 
 // Thread-per-query passes of dense low-dimensional grids (full neighbourhood).
 cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, uint32_t* slot_cell, cudaStream_t st);
