@@ -278,6 +278,7 @@ def _ours(args) -> None:
     import torch.distributed as dist
 
     from gpu_self_join_b200 import JoinConfig, SelfJoin, synth
+    from gpu_self_join_b200.replicas import reduce_step
 
     rank, local_rank, world = _env_rank()
     torch.cuda.set_device(local_rank)
@@ -316,14 +317,7 @@ def _ours(args) -> None:
     ms = e0.elapsed_time(e1)
     R = stats[-1]["total_pairs"]
     pairs_local = R * args.steps
-    ms_max, pairs_all = ms, pairs_local
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        p = torch.tensor([pairs_local], device="cuda", dtype=torch.float64)
-        dist.all_reduce(p, op=dist.ReduceOp.SUM)
-        pairs_all = float(p.item())
+    ms_max, pairs_all = reduce_step(ms, pairs_local, device="cuda")
     value = pairs_all / (ms_max / 1e3)
 
     # ---- roofline of the dominant kernel
@@ -365,11 +359,7 @@ def _ours(args) -> None:
         f1.record()
         torch.cuda.synchronize()
         barrier()
-        ems = f0.elapsed_time(f1)
-        if world > 1:
-            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems, _ = reduce_step(f0.elapsed_time(f1), 0.0, device="cuda")
         e2e = {"value": pairs_all / (ems / 1e3), "unit": "pairs/s", "ms_per_step": ems / args.steps,
                "h2d_bytes_per_step": int(N * n * 4), "d2h_bytes_per_step": int(4 * N + 4 * R)}
 
