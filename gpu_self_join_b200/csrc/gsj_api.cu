@@ -142,7 +142,7 @@ struct gsj_context {
     // device pool
     Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
-        item_off, items, fwd, rev, counts, offsets, revcur, table, temp, scan_temp, misc, var, perm, minarr,
+        item_off, items, fwd, rev, counts, offsets, table, temp, scan_temp, misc, var, perm, minarr,
         minmax_part, pairs, pairs2, srows, snorms, spartial, scentre, unc, table2, nbtab;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
@@ -358,7 +358,7 @@ int pairs_to_csr(gsj_context* c, unsigned long long* pairs, uint64_t nsort, uint
 }
 
 // ------------------------------------------------------------------ warp join (emit)
-// The warp-per-item traversal in one pass: k_join's pass kEmit appends every
+// The warp-per-item traversal in one pass: k_join appends every
 // pair as a packed key (sampling pass over every kSampleStride-th item to size
 // the buffer; a short buffer is re-sized exactly and the pass repeated), then
 // the keys are sorted into the table.
@@ -389,7 +389,7 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
     o.emit = false;
     o.stride = kSampleStride;
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_join<T>(a, kEmit, model, stamp, rows, c->num_sms, st, &o, nsample));
+    GSJ_CUDA(c, launch_join_emit<T>(a, o, nsample, model, stamp, rows, c->num_sms, st));
     unsigned long long sampled = 0;
     GSJ_TRY(d2h_small(c, &sampled, o.rechecks, 1));
     const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
@@ -404,7 +404,7 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
         o.pairs = pairs;
         o.cap = cap;
         S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_join<T>(a, kEmit, model, stamp, rows, c->num_sms, st, &o, ni));
+        GSJ_CUDA(c, launch_join_emit<T>(a, o, ni, model, stamp, rows, c->num_sms, st));
         GSJ_TRY(d2h_small(c, &used, cursor, 1));
         GSJ_TRY(d2h_small(c, &R, o.rechecks, 1));
         if (used <= cap) break;
@@ -853,18 +853,13 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
         return emit_join<T>(c, a, N, stamp, model, rows, counts, offsets, cursor, t_join, t_start);
     }
-    // On the row-range path the distance work is cheap, so the fill pass walks
-    // the full neighbourhood and writes every list forward only (contiguous,
-    // deterministic); the count pass keeps the unicomp traversal of STAMP.  The
-    // pair set is the same either way.
-    const bool fill_stamp = stamp && !rows;
+    // Dense low-dimensional grids (the thread-per-query rows): the distance
+    // work is cheap and the cells too small for per-cell warp work, so one
+    // thread per query counts its full neighbourhood, and the fill pass writes
+    // every list forward only (contiguous, deterministic).
     GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
     S.kernel_launches += 1;
-    // Dense low-dimensional grids count with one thread per query (the full
-    // neighbourhood; the cells there are too small for per-cell warp work);
-    // everything else counts with the warp-per-cell kernel.
-    if (tpq) GSJ_CUDA(c, launch_count_tpq<T>(a, slot_cell, c->num_sms, st));
-    else GSJ_CUDA(c, launch_join<T>(a, kCount, model, stamp, rows, c->num_sms, st));
+    GSJ_CUDA(c, launch_count_tpq<T>(a, slot_cell, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
 
     // ---- list lengths and offsets
@@ -881,26 +876,18 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     S.candidates = ncand;
 
     // ---- fill pass
-    unsigned long long* revcur = nullptr;
     uint32_t* table = nullptr;
-    GSJ_TRY(dev_get(c, c->revcur, N, &revcur));
     GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
-    if (fill_stamp) {
-        S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_rev_cursor(offsets, fwd, ids, N, revcur, st));
-    }
     GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st));
     a.offsets = offsets;
-    a.rev_cursor = revcur;
     a.table = table;
     a.table_cap = R;
     a.err_flag = ctr + 1;  // zeroed with the counters before the count pass
     GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
     S.kernel_launches += 1;
-    // Dense low-dimensional grids fill with a warp per 32 consecutive query
-    // slots (consecutive queries share their cell's candidate tiles).
-    if (tpq) GSJ_CUDA(c, launch_fill_q32<T>(a, slot_cell, c->num_sms, st));
-    else GSJ_CUDA(c, launch_join<T>(a, kFill, model, fill_stamp, rows, c->num_sms, st));
+    // a warp per 32 consecutive query slots (consecutive queries share their
+    // cell's candidate tiles)
+    GSJ_CUDA(c, launch_fill_q32<T>(a, slot_cell, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
     GSJ_CUDA(c, cudaStreamSynchronize(st));
     {
@@ -934,7 +921,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     }
     S.ms_join = now_ms() - t_join;
     S.total_pairs = R;
-    S.join_path = tpq ? GSJ_PATH_ROWS : GSJ_PATH_WARP;
+    S.join_path = GSJ_PATH_ROWS;
     c->R = R;
     c->have_result = true;
     S.ms_total = now_ms() - t_start;
@@ -1022,7 +1009,7 @@ int gsj_destroy(gsj_context* c) {
                    &c->hvals,
                    &c->order,    &c->sizes,
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
-                   &c->revcur,   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
+                   &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
                    &c->minarr,   &c->minmax_part, &c->pairs, &c->pairs2, &c->srows, &c->snorms,
                    &c->spartial, &c->scentre, &c->unc, &c->table2, &c->nbtab};
     for (Buf* b : bufs)

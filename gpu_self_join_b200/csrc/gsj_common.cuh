@@ -18,8 +18,6 @@ constexpr uint64_t kEmptyKey = ~0ull;        // hash table empty slot
 //   kIlpSc  ILP>0,  SHORTCIRCUIT=1  per ILP block: s = fma(d_l, d_l, s); s += d_{l+j}^2 (j >= 1)
 enum Model : int { kSeq = 0, kIlp = 1, kIlpSc = 2 };
 
-enum Pass : int { kCount = 0, kFill = 1, kEmit = 2 };
-
 // Grid geometry (k <= kMaxK indexed dims).
 struct GridGeom {
     uint32_t k;
@@ -50,13 +48,12 @@ struct JoinArgs {
     T thr;                        // s <= thr  <=>  sqrt(s) <= eps
     T eps;                        // epsilon in T (cell formula)
     T minv[kMaxK];                // minArr (grid origin per indexed dim)
-    // count pass
+    // counts (thread-per-query rows; the emit join adds to cand_cnt only)
     uint32_t* fwd_cnt;            // [N] by slot
     uint32_t* rev_cnt;            // [N] by slot (unicomp reverse hits)
     unsigned long long* cand_cnt; // candidate evaluations
-    // fill pass
+    // fill pass (thread-per-query rows)
     const uint64_t* offsets;      // [N+1] by original id
-    unsigned long long* rev_cursor;  // [N] next free reverse entry, by slot
     uint32_t* table;              // [R]
     unsigned long long table_cap; // R: writes at or beyond it are dropped and flagged
     uint32_t* err_flag;           // set to 1 when a write would leave the table

@@ -259,13 +259,6 @@ __global__ void k_sum_counts(const uint32_t* __restrict__ fwd, const uint32_t* _
     if (s < N) total[ids[s]] = fwd[s] + rev[s];
 }
 
-// Reverse-entry cursors by slot: the reverse part of a list follows its forward part.
-__global__ void k_rev_cursor(const uint64_t* __restrict__ offsets, const uint32_t* __restrict__ fwd,
-                             const uint32_t* __restrict__ ids, uint64_t N, unsigned long long* __restrict__ cur) {
-    const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (s < N) cur[s] = offsets[ids[s]] + fwd[s];
-}
-
 // ------------------------------------------------------------ launchers
 static inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
@@ -336,12 +329,6 @@ cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st) {
 cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, const uint32_t* ids, uint64_t N,
                               uint32_t* total, cudaStream_t st) {
     k_sum_counts<<<blocks_for(N, 256), 256, 0, st>>>(fwd, rev, ids, N, total);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, const uint32_t* ids, uint64_t N,
-                              unsigned long long* cur, cudaStream_t st) {
-    k_rev_cursor<<<blocks_for(N, 256), 256, 0, st>>>(offsets, fwd, ids, N, cur);
     return cudaGetLastError();
 }
 

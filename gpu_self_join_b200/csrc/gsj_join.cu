@@ -15,13 +15,12 @@
 //      lane (rows are contiguous in the cell-sorted layout), and tests every
 //      query against the 32 candidates with the reference's exact arithmetic
 //      (s <= thr is sqrt(s) <= eps, see gsj_threshold_*).
-// Pass kCount counts hits per query (and, with STAMP, reverse hits per
-// candidate).  Pass kFill recomputes and writes each hit straight into its
-// final neighbour-table position: forward hits of query j land contiguously
-// at a warp-uniform cursor (ballot + popc, one coalesced store per hit),
-// reverse hits of a candidate are placed through one atomic reservation per
-// (candidate, work item).  No pair buffer and no key sort are needed
-// (kernel.cu:367-375 + GPU.cu:863-980 in the reference).
+// Every hit becomes a packed (query id, candidate id) key appended to the pair
+// buffer (emit_keys), with STAMP also the reverse key of a hit in another cell
+// (the reference emits (q,c) twice there, kernel.cu:367-375); the buffer is
+// sorted into the neighbour table afterwards (the reference's pair buffers +
+// sort_by_key, GPU.cu:863-980).  One traversal per join; a sampling run over
+// every stride-th item sizes the buffer first.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -65,7 +64,7 @@ __host__ __device__ inline WarpSmem warp_smem_layout(uint32_t npad, uint32_t tsi
     return w;
 }
 
-// Pass kEmit: the warp appends its hits as packed (query id << shift |
+// The warp appends its hits as packed (query id << shift |
 // candidate id) keys, and with unicomp the reverse key of a hit in another
 // cell, into blocks of kEmitBlk entries it reserves on o.cursor (unused tails
 // padded with kUndecidedPad, which sorts after every key); emitted counts the
@@ -95,7 +94,32 @@ __device__ __forceinline__ void emit_keys(const TileOut& o, unsigned long long& 
     blk_used += cnt;
 }
 
-template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS, bool ROWS>
+// Slot of candidate f = f0 + lane in the concatenated neighbour ranges
+// (nb_pref: exclusive prefix of the range sizes, nb_pref[nnb] = total).  `ent`
+// is the range holding f0 (warp-uniform).  Every range holds at least one
+// candidate, so the warp's 32 candidates lie in ranges ent .. ent + 31: lane j
+// loads nb_pref[ent + j] and each lane finds its range with a 5-step search
+// over those values; `ent` then moves to the range of f0 + 32 (at most one
+// range past lane 31's).
+__device__ __forceinline__ uint32_t cand_slot(const uint32_t* nb_start, const uint32_t* nb_pref, uint32_t nnb,
+                                              uint32_t& ent, uint32_t f0, uint32_t lane, uint32_t total) {
+    const unsigned FULL = 0xffffffffu;
+    const uint32_t f = f0 + lane;
+    const uint32_t p = ent + lane <= nnb ? nb_pref[ent + lane] : 0xffffffffu;
+    uint32_t lo = 0;
+#pragma unroll
+    for (uint32_t step = 16; step >= 1; step >>= 1) {
+        const uint32_t c = lo + step;
+        if (__shfl_sync(FULL, p, c) <= f) lo = c;
+    }
+    const uint32_t my = ent + lo;
+    const uint32_t pf = __shfl_sync(FULL, p, lo);
+    const uint32_t e31 = __shfl_sync(FULL, my, 31);
+    ent = (e31 + 1u <= nnb && nb_pref[e31 + 1u] <= f0 + 32u) ? e31 + 1u : e31;
+    return f < total ? nb_start[my] + (f - pf) : 0u;
+}
+
+template <typename T, int NT, int MODEL, int POL, bool STAMP, bool ROWS>
 __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff,
                                               uint32_t batch, const TileOut o, uint32_t nvisit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -114,7 +138,7 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
     const unsigned lt = lanemask_lt();
     const uint32_t k = a.g.k;
     unsigned long long cand_total = 0;
-    unsigned long long blk_base = 0, emitted = 0;  // pass kEmit
+    unsigned long long blk_base = 0, emitted = 0;
     uint32_t blk_used = kEmitBlk;
 
     // work items are claimed `batch` at a time (one atomic per batch); item i
@@ -214,99 +238,51 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
         for (uint32_t e = lane; e < qn * npad; e += 32) q_s[e] = a.pts[(size_t)q0 * npad + e];
         if (lane < qn) qid_s[lane] = a.ids[q0 + lane];
         __syncwarp();
-        if (PASS != kFill) cand_total += (unsigned long long)total * qn;
-        uint32_t myq = 0;                 // count pass: lane j holds query j's forward count
-        unsigned long long mycur = 0;     // fill pass: lane j holds query j's next table position
-        if (PASS == kFill && lane < qn) mycur = a.offsets[qid_s[lane]];
-        const uint64_t my_qid = lane < qn ? qid_s[lane] : 0u;  // pass kEmit
+        cand_total += (unsigned long long)total * qn;
+        const uint64_t my_qid = lane < qn ? qid_s[lane] : 0u;
 
         if constexpr (!GENERIC) {
             // ---- register path (n <= 8): up to G tiles of 32 candidates live in
             // registers; queries outside, tiles inside, so each query's
-            // cursor and coordinates are loaded once per group of tiles.
+            // coordinates are loaded once per group of tiles.
             constexpr int G = 4;
             constexpr int NR = NT > 0 ? NT : 1;
             uint32_t ent = 0;
             for (uint32_t g0 = 0; g0 < total; g0 += 32u * G) {
                 T cx[G][NR];
-                uint32_t cid[G], cslot[G];
+                uint32_t cid[G];
                 bool cval[G], ccross[G];
                 const uint32_t ntile = min((uint32_t)G, (total - g0 + 31u) / 32u);
 #pragma unroll
                 for (int t = 0; t < G; t++) {
                     const uint32_t f = g0 + (uint32_t)t * 32u + lane;
                     cval[t] = f < total;
-                    cslot[t] = 0u;
                     cid[t] = 0u;
                     ccross[t] = false;
                     if ((uint32_t)t >= ntile) continue;
-                    uint32_t slot = 0;
-                    if (cval[t]) {
-                        while (nb_pref[ent + 1] <= f) ent++;
-                        slot = nb_start[ent] + (f - nb_pref[ent]);
-                    }
-                    cslot[t] = slot;
-                    ccross[t] = STAMP && cval[t] && (slot < cs || slot >= ce);
-                    cid[t] = (PASS != kCount && cval[t]) ? a.ids[slot] : 0u;
+                    const uint32_t slot = cand_slot(nb_start, nb_pref, nnb, ent, g0 + (uint32_t)t * 32u, lane, total);
+                    if (cval[t]) cid[t] = a.ids[slot];
+                    ccross[t] = STAMP && cval[t] && (slot < cs || slot >= ce);  // outside the own cell
                     const T* row = a.pts + (size_t)slot * npad;
 #pragma unroll
                     for (int l = 0; l < NR; l++) cx[t][l] = row[l];
                 }
-                uint32_t rev[G], revmask[G];
-#pragma unroll
-                for (int t = 0; t < G; t++) rev[t] = revmask[t] = 0u;
                 for (uint32_t j = 0; j < qn; j++) {
                     T q[NR];
 #pragma unroll
                     for (int l = 0; l < NR; l++) q[l] = q_s[(size_t)j * npad + l];
-                    uint32_t cntj = 0;
-                    unsigned long long cur = 0;
-                    if (PASS == kFill) cur = __shfl_sync(FULL, mycur, j);
+                    const uint64_t qid = __shfl_sync(FULL, my_qid, j);
 #pragma unroll
                     for (int t = 0; t < G; t++) {
                         if ((uint32_t)t < ntile) {
                             const T s = sqdist_seq_reg<T, NR, POL>(q, cx[t]);
                             const bool hit = cval[t] && (s <= a.thr);
                             const unsigned b = __ballot_sync(FULL, hit);
-                            if (PASS == kCount) {
-                                cntj += __popc(b);
-                                if (STAMP && ccross[t] && hit) rev[t]++;
-                            } else if (PASS == kFill) {
-                                if (hit) {
-                                    const unsigned long long pos = cur + __popc(b & lt);
-                                    if (pos < a.table_cap) a.table[pos] = cid[t];
-                                    else *a.err_flag = 1u;
-                                }
-                                cur += __popc(b);
-                                if (STAMP && ccross[t] && hit) revmask[t] |= 1u << j;
-                            } else if (b) {
+                            if (b) {
                                 const bool cr = STAMP && ccross[t] && hit;
                                 const unsigned cb = __ballot_sync(FULL, cr);
-                                emit_keys(o, blk_base, blk_used, emitted, hit, cr, b, cb, lt, lane,
-                                          __shfl_sync(FULL, my_qid, j), cid[t]);
+                                emit_keys(o, blk_base, blk_used, emitted, hit, cr, b, cb, lt, lane, qid, cid[t]);
                             }
-                        }
-                    }
-                    if (PASS == kCount) {
-                        if (lane == (int)j) myq += cntj;
-                    } else if (PASS == kFill) {
-                        if (lane == (int)j) mycur = cur;
-                    }
-                }
-#pragma unroll
-                for (int t = 0; t < G; t++) {
-                    if (PASS == kCount) {
-                        if (STAMP && rev[t]) atomicAdd(&a.rev_cnt[cslot[t]], rev[t]);
-                    } else if (PASS == kFill && STAMP && revmask[t]) {
-                        unsigned long long pos =
-                            atomicAdd(&a.rev_cursor[cslot[t]], (unsigned long long)__popc(revmask[t]));
-                        uint32_t m = revmask[t];
-                        while (m) {
-                            const int j = __ffs(m) - 1;
-                            m &= m - 1u;
-                            if (pos < a.table_cap) a.table[pos] = qid_s[j];
-                            else *a.err_flag = 1u;
-                            pos++;
                         }
                     }
                 }
@@ -317,11 +293,10 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
             for (uint32_t t0 = 0; t0 < total; t0 += 32) {
                 const uint32_t f = t0 + lane;
                 const bool valid = f < total;
-                uint32_t slot = 0, corig = 0;
+                const uint32_t slot = cand_slot(nb_start, nb_pref, nnb, ent, t0, lane, total);
+                uint32_t corig = 0;
                 bool cross = false;
                 if (valid) {
-                    while (nb_pref[ent + 1] <= f) ent++;
-                    slot = nb_start[ent] + (f - nb_pref[ent]);
                     cross = STAMP && (slot < cs || slot >= ce);  // outside the own cell
                     corig = a.ids[slot];
                 }
@@ -331,66 +306,36 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
                     for (uint32_t l = 0; l < a.n; l++) dst[l] = row[l];
                     __syncwarp();
                 }
-                uint32_t myrev = 0, revmask = 0;
                 for (uint32_t j = 0; j < qn; j++) {
                     const T* q = q_s + (size_t)j * npad;
                     const T s =
                         sqdist_generic<T, MODEL, POL>(q, cand_s + (size_t)lane * (npad + 1u), a.n, a.ilp, a.thr, valid);
                     const bool hit = valid && (s <= a.thr);
                     const unsigned b = __ballot_sync(FULL, hit);
-                    if (PASS == kCount) {
-                        if (lane == (int)j) myq += __popc(b);
-                        if (STAMP && cross && hit) myrev++;
-                    } else if (PASS == kEmit) {
-                        if (b) {
-                            const bool cr = STAMP && cross && hit;
-                            const unsigned cb = __ballot_sync(FULL, cr);
-                            emit_keys(o, blk_base, blk_used, emitted, hit, cr, b, cb, lt, lane,
-                                      __shfl_sync(FULL, my_qid, j), corig);
-                        }
-                    } else {
-                        const unsigned long long cur = __shfl_sync(FULL, mycur, j);
-                        if (hit) {
-                            const unsigned long long pos = cur + __popc(b & lt);
-                            if (pos < a.table_cap) a.table[pos] = corig;
-                            else *a.err_flag = 1u;
-                        }
-                        if (lane == (int)j) mycur += __popc(b);
-                        if (STAMP && cross && hit) revmask |= 1u << j;
-                    }
-                }
-                if (PASS == kCount) {
-                    if (STAMP && myrev) atomicAdd(&a.rev_cnt[slot], myrev);
-                } else if (PASS == kFill && STAMP && revmask) {
-                    unsigned long long pos = atomicAdd(&a.rev_cursor[slot], (unsigned long long)__popc(revmask));
-                    while (revmask) {
-                        const int j = __ffs(revmask) - 1;
-                        revmask &= revmask - 1u;
-                        if (pos < a.table_cap) a.table[pos] = qid_s[j];
-                        else *a.err_flag = 1u;
-                        pos++;
+                    if (b) {
+                        const bool cr = STAMP && cross && hit;
+                        const unsigned cb = __ballot_sync(FULL, cr);
+                        emit_keys(o, blk_base, blk_used, emitted, hit, cr, b, cb, lt, lane,
+                                  __shfl_sync(FULL, my_qid, j), corig);
                     }
                 }
                 __syncwarp();
             }
         }
-        if (PASS == kCount && lane < qn) a.fwd_cnt[q0 + lane] = myq;
         __syncwarp();
     }
-    if (PASS != kFill && lane == 0 && cand_total && (PASS == kCount || o.emit)) atomicAdd(a.cand_cnt, cand_total);
-    if (PASS == kEmit) {
-        if (o.emit && blk_used < kEmitBlk)
-            for (uint32_t e = blk_used + (uint32_t)lane; e < kEmitBlk; e += 32u)
-                if (blk_base + e < o.cap) o.pairs[blk_base + e] = kUndecidedPad;
-        if (lane == 0 && emitted) atomicAdd(o.rechecks, emitted);
-    }
+    if (lane == 0 && cand_total && o.emit) atomicAdd(a.cand_cnt, cand_total);
+    if (o.emit && blk_used < kEmitBlk)
+        for (uint32_t e = blk_used + (uint32_t)lane; e < kEmitBlk; e += 32u)
+            if (blk_base + e < o.cap) o.pairs[blk_base + e] = kUndecidedPad;
+    if (lane == 0 && emitted) atomicAdd(o.rechecks, emitted);
 }
 
 // ------------------------------------------------------------------ launch
-template <typename T, int NT, int MODEL, int POL, bool STAMP, int PASS, bool ROWS>
+template <typename T, int NT, int MODEL, int POL, bool STAMP, bool ROWS>
 static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t noff, const TileOut& o,
                               uint32_t nvisit, int num_sms, cudaStream_t st) {
-    auto kern = k_join<T, NT, MODEL, POL, STAMP, PASS, ROWS>;
+    auto kern = k_join<T, NT, MODEL, POL, STAMP, ROWS>;
     const WarpSmem L = warp_smem_layout(a.npad, sizeof(T), nb_cap, NT == 0);
     const uint32_t max_smem = 200u * 1024u;
     int warps = (int)(max_smem / L.total);
@@ -418,74 +363,61 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     return cudaGetLastError();
 }
 
-template <typename T, int MODEL, int POL, bool STAMP, int PASS>
+template <typename T, int MODEL, int POL, bool STAMP>
 static cudaError_t dispatch_nt(const JoinArgs<T>& a, bool rows, uint32_t nb_cap, uint32_t noff, const TileOut& o,
                                uint32_t nvisit, int num_sms, cudaStream_t st) {
     if (rows) {
         // low-dimensional dense grids (k <= 3): registers for n <= 4
         if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
             switch (a.n) {
-                case 1: return launch_one<T, 1, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
-                case 2: return launch_one<T, 2, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
-                case 3: return launch_one<T, 3, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
-                case 4: return launch_one<T, 4, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+                case 1: return launch_one<T, 1, MODEL, POL, STAMP, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+                case 2: return launch_one<T, 2, MODEL, POL, STAMP, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+                case 3: return launch_one<T, 3, MODEL, POL, STAMP, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+                case 4: return launch_one<T, 4, MODEL, POL, STAMP, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
                 default: break;
             }
         }
-        return launch_one<T, 0, MODEL, POL, STAMP, PASS, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
+        return launch_one<T, 0, MODEL, POL, STAMP, true>(a, nb_cap, noff, o, nvisit, num_sms, st);
     }
     if (MODEL == kSeq && a.npad == npad_for(a.n, sizeof(T))) {
         switch (a.n) {
-            case 6: return launch_one<T, 6, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
-            case 8: return launch_one<T, 8, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
+            case 6: return launch_one<T, 6, MODEL, POL, STAMP, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
+            case 8: return launch_one<T, 8, MODEL, POL, STAMP, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
             default: break;
         }
     }
-    return launch_one<T, 0, MODEL, POL, STAMP, PASS, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
+    return launch_one<T, 0, MODEL, POL, STAMP, false>(a, nb_cap, noff, o, nvisit, num_sms, st);
 }
 
-template <typename T, bool STAMP, int PASS>
+template <typename T, bool STAMP>
 static cudaError_t dispatch_model(const JoinArgs<T>& a, int model, bool rows, uint32_t nb_cap, uint32_t noff,
                                   const TileOut& o, uint32_t nvisit, int num_sms, cudaStream_t st) {
     constexpr int P = sizeof(T) == 8 ? kPolF64 : kPolF32;
     switch (model) {
-        case kSeq: return dispatch_nt<T, kSeq, P, STAMP, PASS>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
-        case kIlp: return dispatch_nt<T, kIlp, P, STAMP, PASS>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
-        case kIlpSc: return dispatch_nt<T, kIlpSc, P, STAMP, PASS>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
+        case kSeq: return dispatch_nt<T, kSeq, P, STAMP>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
+        case kIlp: return dispatch_nt<T, kIlp, P, STAMP>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
+        case kIlpSc: return dispatch_nt<T, kIlpSc, P, STAMP>(a, rows, nb_cap, noff, o, nvisit, num_sms, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <typename T>
-cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, bool rows, int num_sms,
-                        cudaStream_t st, const TileOut* emit, uint32_t nvisit) {
+cudaError_t launch_join_emit(const JoinArgs<T>& a, const TileOut& o, uint32_t nvisit, int model, bool stamp, bool rows,
+                             int num_sms, cudaStream_t st) {
     uint32_t noff = 1;
     for (uint32_t j = 0; j < a.g.k; j++) noff *= 3u;
     if (rows && (a.g.k > 3 || !a.ds)) return cudaErrorInvalidValue;
-    const uint32_t nb_cap = rows ? 32u : noff;
-    TileOut o{};
-    o.stride = 1;
-    if (pass == kEmit) {
-        if (!emit || emit->stride == 0) return cudaErrorInvalidValue;
-        o = *emit;
-    } else {
-        nvisit = a.num_items;
-    }
+    if (o.stride == 0) return cudaErrorInvalidValue;
     if (nvisit == 0) return cudaSuccess;
     if ((uint64_t)(nvisit - 1) * o.stride >= a.num_items) return cudaErrorInvalidValue;
-    if (pass == kCount)
-        return stamp ? dispatch_model<T, true, kCount>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st)
-                     : dispatch_model<T, false, kCount>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st);
-    if (pass == kEmit)
-        return stamp ? dispatch_model<T, true, kEmit>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st)
-                     : dispatch_model<T, false, kEmit>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st);
-    return stamp ? dispatch_model<T, true, kFill>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st)
-                 : dispatch_model<T, false, kFill>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st);
+    const uint32_t nb_cap = rows ? 32u : noff;
+    return stamp ? dispatch_model<T, true>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st)
+                 : dispatch_model<T, false>(a, model, rows, nb_cap, noff, o, nvisit, num_sms, st);
 }
 
-template cudaError_t launch_join<float>(const JoinArgs<float>&, int, int, bool, bool, int, cudaStream_t,
-                                        const TileOut*, uint32_t);
-template cudaError_t launch_join<double>(const JoinArgs<double>&, int, int, bool, bool, int, cudaStream_t,
-                                         const TileOut*, uint32_t);
+template cudaError_t launch_join_emit<float>(const JoinArgs<float>&, const TileOut&, uint32_t, int, bool, bool, int,
+                                             cudaStream_t);
+template cudaError_t launch_join_emit<double>(const JoinArgs<double>&, const TileOut&, uint32_t, int, bool, bool, int,
+                                              cudaStream_t);
 
 }  // namespace gsj

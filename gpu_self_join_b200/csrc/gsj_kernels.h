@@ -64,19 +64,17 @@ cudaError_t launch_make_items(const uint32_t* order, const uint32_t* nchunks, co
 cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st);
 cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, const uint32_t* ids, uint64_t N,
                               uint32_t* total, cudaStream_t st);
-cudaError_t launch_rev_cursor(const uint64_t* offsets, const uint32_t* fwd, const uint32_t* ids, uint64_t N,
-                              unsigned long long* cur, cudaStream_t st);
 
-// Join passes.  `pass` is kCount or kFill; `model` one of Model; `stamp`
-// selects the unicomp traversal.  The launcher picks the specialisation.
-// `rows` selects the dense low-dimensional specialisation (k <= 3, a.ds set).
-// Pass kEmit appends packed pair keys into *emit (TileOut; its rechecks
-// counter receives the exact number of keys) and visits items 0, stride, ...,
-// (nvisit - 1) * stride; the other passes visit every item.
+// The warp-per-item join: appends packed pair keys into `o` (its rechecks
+// counter receives the exact number of keys; with o.emit false only that
+// count is taken) and visits items 0, o.stride, ..., (nvisit - 1) * o.stride.
+// `model` is one of Model; `stamp` selects the unicomp traversal; `rows` the
+// dense low-dimensional specialisation (k <= 3, a.ds set).  The launcher picks
+// the specialisation.
 struct TileOut;
 template <typename T>
-cudaError_t launch_join(const JoinArgs<T>& a, int pass, int model, bool stamp, bool rows, int num_sms,
-                        cudaStream_t st, const TileOut* emit = nullptr, uint32_t nvisit = 0);
+cudaError_t launch_join_emit(const JoinArgs<T>& a, const TileOut& o, uint32_t nvisit, int model, bool stamp, bool rows,
+                             int num_sms, cudaStream_t st);
 
 // Thread-per-query passes of dense low-dimensional grids (full neighbourhood).
 cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, uint32_t* slot_cell, cudaStream_t st);

@@ -156,6 +156,45 @@ def test_screen_with_nonfinite_points(oracle, stamp):
     assert st["screen_rechecks"] < st["candidates"] // 4
 
 
+@pytest.mark.parametrize("n", [6, 16, 18, 126])
+def test_tiny_and_degenerate_inputs(oracle, n):
+    """One point, eight identical points (one cell: the tile and screen paths
+    with a single item) and exact duplicates at every dimensionality the
+    paths switch on."""
+    c, t, _ = run_gpu(np.full((1, n), 0.5, dtype=np.float32), 0.5, indexed_dims=6)
+    assert list(c) == [1] and list(t) == [0]
+    c, t, st = run_gpu(np.full((8, n), 2.0, dtype=np.float32), 0.5, indexed_dims=6, stamp=True)
+    assert list(c) == [8] * 8 and st["total_pairs"] == 64
+    # lattice points (distinct ones at least 1 apart), 40 cells per indexed dim
+    rng = np.random.default_rng(40 + n)
+    base = rng.integers(0, 20, size=(300, n)).astype(np.float32)
+    pts = np.concatenate([base, base, base[:50]])
+    assert_same(oracle, pts, 0.5, indexed_dims=6)
+
+
+@pytest.mark.parametrize("n", [16, 126])
+def test_screen_dimension_bounds(oracle, n):
+    """The smallest and the largest dimensionality the tensor-core screen
+    takes (n + 2 columns, the folded norm, within one 128-wide tile)."""
+    pts = tile_points(n, 6000, 3.0, 300 + n)
+    st = assert_same(oracle, pts, 3.0, indexed_dims=6, stamp=(n == 16))
+    assert st["join_path"] == 3
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("stamp", [False, True])
+def test_warp_path_sparse_cells(oracle, dtype, stamp):
+    """Mostly one point per cell in 6 indexed dims: a warp's 32 candidates
+    come from up to 32 different neighbour ranges (the candidate-slot search
+    across ranges), mixed with a few dense cells of many ranges' worth."""
+    rng = np.random.default_rng(21)
+    sparse = rng.uniform(0, 5, size=(15000, 7))  # about one point per cell, ~460 non-empty neighbours
+    dense = rng.uniform(0, 1.5, size=(3000, 7)) + 2.0
+    pts = np.concatenate([sparse, dense]).astype(dtype)[rng.permutation(18000)]
+    st = assert_same(oracle, pts, 1.0, indexed_dims=6, stamp=stamp)
+    assert st["join_path"] == 0  # GSJ_PATH_WARP
+
+
 def test_tile_join_deterministic():
     pts = tile_points(18, 20000, 3.0, 7)
     c1, t1, s1 = run_gpu(pts, 3.0, indexed_dims=6, stamp=True)
