@@ -112,6 +112,19 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _tensor_peak():
+    """Dense BF16 tensor peak: the sustained (power-capped) figure, since the
+    screen runs inside joins of hundreds of milliseconds, back to back."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        v = d.get("bf16_tflops_sustained", d.get("bf16_tflops"))
+        if v is not None:
+            return float(v), "measured"
+    return 1400.0, "fallback (sustained)"
+
+
 def _traffic_from_profile(kernel: str, workload: str):
     """DRAM bytes per launch recorded from an ncu capture in profiles/."""
     p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
@@ -125,6 +138,49 @@ def _traffic_from_profile(kernel: str, workload: str):
                 except ValueError:
                     return None
     return None
+
+
+def _roofline(stats: list, N: int, n: int, R: int, w) -> dict:
+    """Roofline object for the join's dominant stage.  The device clock
+    brackets two stages per join: "count" (ROWS: the count pass; the other
+    paths: sampling + the pair-emitting join) and "fill" (ROWS: the fill pass;
+    the other paths: pair sort + table).  Algorithmic bytes per launch:
+      join_fill   coordinates 4Nn + ids 4N + offsets 8N + table 4R
+      join_count  coordinates 4Nn + ids 4N + counts 4N (+ reverse counts 4N with STAMP)
+      join_emit   coordinates 4Nn + ids 4N + 8-byte pair keys 8R
+      pair_sort   keys 8R read + table 4R + offsets 8N written
+    The screen is a tensor-core kernel: 2(n+2) FLOPs per screened pair (one
+    dot product of the n centred coordinates and the two norm columns)."""
+    fill_ms = statistics.mean(s["dev_ms_fill"] for s in stats)
+    count_ms = statistics.mean(s["dev_ms_count"] for s in stats)
+    path = int(stats[-1].get("join_path", 1))
+    peak, peak_kind = _peaks()
+    b_coords = 4.0 * N * n
+    bound, unit, pk = "hbm", "GB/s", peak
+    if path == 1:  # GSJ_PATH_ROWS
+        work_fill = b_coords + 4.0 * N + 8.0 * N + 4.0 * R
+        work_count = b_coords + 4.0 * N + 4.0 * N + (4.0 * N if w.stamp else 0.0)
+        names = ("join_fill", "join_count")
+    else:
+        work_fill = 8.0 * R + 4.0 * R + 8.0 * N
+        work_count = b_coords + 4.0 * N + 8.0 * R
+        names = ("pair_sort", "join_emit")
+    if fill_ms >= count_ms:
+        kname, kms, kwork = names[0], fill_ms, work_fill
+    else:
+        kname, kms, kwork = names[1], count_ms, work_count
+        if path == 3:  # GSJ_PATH_SCREEN
+            kname, bound, unit = "tile_screen", "tensor", "TFLOP/s"
+            kwork = 2.0 * (n + 2) * float(stats[-1]["candidates"])
+            pk, peak_kind = _tensor_peak()
+    achieved = kwork / (kms / 1e3) / (1e12 if unit == "TFLOP/s" else 1e9)
+    roof = {"bound": bound, "kernel": kname, "achieved": achieved, "peak": pk, "unit": unit,
+            "frac": achieved / pk, "peak_source": peak_kind,
+            ("algorithmic_flops" if unit == "TFLOP/s" else "algorithmic_bytes"): kwork,
+            "kernel_ms": kms, "traffic": _traffic_from_profile(kname, w.name),
+            "stage_ms": {"index": statistics.mean(s["dev_ms_index"] for s in stats), "count": count_ms,
+                         "fill": fill_ms}}
+    return roof
 
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "rtree_harness")
@@ -321,22 +377,7 @@ def _ours(args) -> None:
     value = pairs_all / (ms_max / 1e3)
 
     # ---- roofline of the dominant kernel
-    fill_ms = statistics.mean(s["dev_ms_fill"] for s in stats)
-    count_ms = statistics.mean(s["dev_ms_count"] for s in stats)
-    peak, peak_kind = _peaks()
-    b_coords = 4.0 * N * n
-    bytes_fill = b_coords + 4.0 * N + 8.0 * N + 4.0 * R
-    bytes_count = b_coords + 4.0 * N + 4.0 * N + (4.0 * N if w.stamp else 0.0)
-    if fill_ms >= count_ms:
-        kname, kms, kbytes = "join_fill", fill_ms, bytes_fill
-    else:
-        kname, kms, kbytes = "join_count", count_ms, bytes_count
-    achieved = kbytes / (kms / 1e3) / 1e9
-    roof = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "algorithmic_bytes": kbytes,
-            "kernel_ms": kms, "traffic": _traffic_from_profile(kname, args.workload),
-            "stage_ms": {"index": statistics.mean(s["dev_ms_index"] for s in stats), "count": count_ms,
-                         "fill": fill_ms}}
+    roof = _roofline(stats, N, n, R, w)
 
     # ---- e2e: host buffers through the public API
     e2e = None
