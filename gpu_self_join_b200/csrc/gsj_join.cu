@@ -121,7 +121,7 @@ __device__ __forceinline__ uint32_t cand_slot(const uint32_t* nb_start, const ui
 
 template <typename T, int NT, int MODEL, int POL, bool STAMP, bool ROWS>
 __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff,
-                                              uint32_t batch, const TileOut o, uint32_t nvisit) {
+                                              const TileOut o, uint32_t nvisit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool GENERIC = (NT == 0);
     const unsigned FULL = 0xffffffffu;
@@ -141,19 +141,20 @@ __global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_c
     unsigned long long blk_base = 0, emitted = 0;
     uint32_t blk_used = kEmitBlk;
 
-    // work items are claimed `batch` at a time (one atomic per batch); item i
-    // is items[i * o.stride] (a stride above 1 samples every stride-th item)
-    uint32_t item = 0, item_end = 0;
+    // Work items are claimed one at a time: items in cell order are as heavy
+    // as their cells are dense, so claiming runs of consecutive items left one
+    // warp with a run of the densest cells long after the others had finished
+    // (on a 5M-point 6-D Gaussian mixture the heaviest run of 32 items held 7.5x
+    // a warp's mean share).  The next claim is issued before the current item
+    // is processed and read after it, so its latency hides behind the item.
+    // Item i is items[i * o.stride] (a stride above 1 samples every stride-th item).
+    uint32_t claim = 0;
+    if (lane == 0) claim = atomicAdd(a.work_counter, 1u);
     for (;;) {
-        if (item >= item_end) {
-            uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(a.work_counter, batch);
-            base = __shfl_sync(FULL, base, 0);
-            if (base >= nvisit) break;
-            item = base;
-            item_end = min(base + batch, nvisit);
-        }
-        const uint2 wi = a.items[(size_t)(item++) * o.stride];
+        const uint32_t item = __shfl_sync(FULL, claim, 0);
+        if (item >= nvisit) break;
+        if (lane == 0) claim = atomicAdd(a.work_counter, 1u);
+        const uint2 wi = a.items[(size_t)item * o.stride];
         const uint32_t cell = wi.x;
         const uint32_t cs = a.cell_start[cell], ce = a.cell_start[cell + 1];
         const uint32_t q0 = cs + wi.y * kQChunk;
@@ -356,10 +357,10 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     const uint64_t needed = ((uint64_t)nvisit + warps - 1) / warps;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > needed) blocks = needed ? needed : 1;
+    // every warp claims once past the last item: the counter must not wrap
     const uint64_t total_warps = blocks * (uint64_t)warps;
-    uint64_t batch = nvisit / (total_warps * 16u);
-    batch = batch < 1 ? 1 : (batch > 32 ? 32 : batch);
-    kern<<<(unsigned)blocks, threads, smem, st>>>(a, nb_cap, noff, (uint32_t)batch, o, nvisit);
+    if ((uint64_t)nvisit + total_warps >= 0xffffffffull) return cudaErrorInvalidValue;
+    kern<<<(unsigned)blocks, threads, smem, st>>>(a, nb_cap, noff, o, nvisit);
     return cudaGetLastError();
 }
 
