@@ -83,13 +83,14 @@ typedef struct gsj_stats {
     uint64_t work_items;      /* scheduled (query cell chunk) work items        */
     double ms_h2d;            /* host->device copy of the dataset               */
     double ms_index;          /* REORDER + grid extents + on-device index build */
-    double ms_join;           /* count pass + offsets + fill pass               */
+    double ms_join;           /* join: count + offsets + fill (ROWS), or pair
+                                 emission + pair sort + table (other paths)     */
     double ms_d2h;            /* result copies to the host                      */
     double ms_total;          /* whole call                                     */
     /* device time (CUDA events on the context's stream) */
     double dev_ms_index;      /* index build: keys, sort, cells, lookup, items  */
-    double dev_ms_count;      /* count pass (tile join: the distance pass)      */
-    double dev_ms_fill;       /* fill pass (tile join: pair sort + table)       */
+    double dev_ms_count;      /* count pass (other paths: the distance pass)    */
+    double dev_ms_fill;       /* fill pass (other paths: pair sort + table)     */
     uint64_t kernel_launches; /* launches of this library's own kernels         */
     uint64_t join_path;       /* GSJ_PATH_* taken by the last join              */
     uint64_t screen_rechecks; /* GSJ_PATH_SCREEN: pairs the BF16 screen could not
@@ -97,7 +98,7 @@ typedef struct gsj_stats {
 } gsj_stats;
 
 /* Join paths (gsj_stats.join_path). */
-#define GSJ_PATH_WARP 0u  /* warp per (cell, 32 queries): count pass + fill pass   */
+#define GSJ_PATH_WARP 0u  /* warp per (cell, 32 queries): pair keys + on-device sort */
 #define GSJ_PATH_ROWS 1u  /* dense k <= 3, n <= 4: thread-per-query count + fill   */
 #define GSJ_PATH_TILE 2u  /* float, 5 <= n <= 128, k <= 6, >= 8 points per cell:
                              64 x 64 register tiles, pair buffer, on-device sort */
