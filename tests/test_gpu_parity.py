@@ -193,6 +193,10 @@ def test_warp_path_sparse_cells(oracle, dtype, stamp):
     pts = np.concatenate([sparse, dense]).astype(dtype)[rng.permutation(18000)]
     st = assert_same(oracle, pts, 1.0, indexed_dims=6, stamp=stamp)
     assert st["join_path"] == 0  # GSJ_PATH_WARP
+    # lists come out of the pair sort ascending
+    c, t, _ = run_gpu(pts, 1.0, indexed_dims=6, stamp=stamp)
+    starts = np.concatenate([[0], np.cumsum(c.astype(np.int64))])
+    assert all(np.all(np.diff(t[starts[i]:starts[i + 1]].astype(np.int64)) > 0) for i in range(0, c.size, 61))
 
 
 def test_tile_join_deterministic():
