@@ -8,7 +8,10 @@
 //     with the reference comparator, main.cu:1040)
 //   grid extents: device min/max, scalar tail on the host (main.cu:925-946)
 //   index: cell keys -> radix sort -> runs -> cell table -> work items
-//   count pass -> list offsets (scan) -> fill pass  (the neighbour table)
+//   join, one of four paths (gsj_stats.join_path):
+//     ROWS   (dense, k <= 3, n <= 4): count pass -> list offsets -> fill pass
+//     WARP, TILE, SCREEN: one pass appending packed (query, candidate) keys,
+//       sized by a sampling pass -> radix sort -> table + offsets
 // The result stays on the device in the context's pool until fetched.
 #include <cuda_runtime.h>
 
@@ -807,7 +810,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     const double t_join = now_ms();
     S.ms_index = t_join - t_index;
 
-    // ---- count pass
+    // ---- join arguments (every path); per-slot counts for the ROWS count pass
     uint32_t *fwd = nullptr, *rev = nullptr;
     GSJ_TRY(dev_get(c, c->fwd, N, &fwd));
     GSJ_TRY(dev_get(c, c->rev, N, &rev));
