@@ -58,6 +58,12 @@
 #ifndef STAMP
 #define STAMP 0
 #endif
+// LINEARSTAMP (kernel.cu:272-289) visits the own cell and the neighbour cells
+// of larger linear id: another half of the cross-cell pairs than STAMP's
+// parity rule, the same pair set.  It selects the unicomp traversal here.
+#ifndef LINEARSTAMP
+#define LINEARSTAMP 0
+#endif
 #ifndef QUERYREORDER
 #define QUERYREORDER 0
 #endif
@@ -965,7 +971,7 @@ void gsj_default_config(gsj_config* cfg) {
     cfg->reorder = REORDER;
     cfg->shortcircuit = SHORTCIRCUIT;
     cfg->ilp = ILP;
-    cfg->stamp = STAMP;
+    cfg->stamp = (STAMP || LINEARSTAMP) ? 1 : 0;
     cfg->query_reorder = QUERYREORDER;
     cfg->device = 0;
     cfg->flags = GSJ_FLAG_QUIET;
