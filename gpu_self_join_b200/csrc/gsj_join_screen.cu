@@ -32,10 +32,10 @@
 // The emitted pair set is the plain path's, bit for bit.  Non-finite values
 // only make the test inconclusive, which sends the pair to the exact check.
 //
-// Synchronisation: warps 4-7 produce candidate tiles (slot search, cp.async of
-// the rows) and issue the MMA, warps
-// 0-3 consume; two tiles and two accumulators alternate, handed over by
-// mbarriers (full: MMA commit + the issuer's release; empty: 128 consumer
+// Synchronisation: warps 8-11 produce candidate tiles (slot search, cp.async of
+// the rows) and issue the MMA, warps 0-7 consume; candidate tiles rotate
+// through kStages buffers and two accumulators alternate, handed over by
+// mbarriers (full: MMA commit + the issuer's release; empty: the consumer
 // arrivals).  Every wait is a bounded poll by one thread whose verdict is
 // shared before any barrier or warp-collective; on time-out the error flag is
 // raised and the CTA stops.  Tensor memory (2 x 128 columns) is allocated once
@@ -274,15 +274,15 @@ __device__ __forceinline__ bool named_sync_or(uint32_t id, uint32_t count, bool 
     return r != 0u;
 }
 
-// The CTA is warp-specialised: warps 4-7 produce (candidate slots, centred
-// BF16 candidate tile with the norm folded in, the MMA), warps 0-3 consume
-// (tensor-memory rows, the screen, the exact check, the pair appends).  Two
-// candidate tiles and two accumulators alternate; mbarriers full[s] (MMA done)
-// and empty[s] (accumulator read) hand them over.
+// The CTA is warp-specialised: warps 8-11 produce (candidate slots, centred
+// BF16 candidate rows with the norm folded in, the MMA), warps 0-7 consume
+// (tensor-memory rows, the screen, the undecided-pair appends).  Candidate
+// tiles rotate through kStages buffers and two accumulators alternate;
+// mbarriers full[s] (MMA done) and empty[s] (accumulator read) hand them over.
 //
-// With the norm folded into the product (A row = [q^, 1, 1], B row =
-// [-2 c^, |c^|^2_hi, |c^|^2_lo]), the accumulator holds |c^_j|^2 - 2 q^_i.c^_j
-// directly and the screen is one comparison per pair.
+// With the norm folded into the product (A row, the query = [-2 q^, 1, 1];
+// B row, the candidate = [c^, |c^|^2_hi, |c^|^2_lo]), the accumulator holds
+// |c^_j|^2 - 2 q^_i.c^_j directly and the screen is one comparison per pair.
 template <int MODEL, bool STAMP>
 __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<float> a, const TileOut o,
                                                               const ScreenConst sc, uint32_t noff, uint32_t nvisit) {

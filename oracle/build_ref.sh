@@ -15,9 +15,10 @@
 # The binaries are test infrastructure: the oracle's pin against the reference
 # (tests/golden/make_ref_fixtures.py) and the reference arm of bench.py.
 #
-# usage: oracle/build_ref.sh [REFERENCE_DIR]    (default /root/reference)
+# usage: oracle/build_ref.sh [REFERENCE_DIR]
+#   (default: $GSJ_REFERENCE_DIR, else the checkout at /root/reference)
 set -euo pipefail
-REF=${1:-/root/reference}
+REF=${1:-${GSJ_REFERENCE_DIR:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 [ -d "$REF" ] || { echo "reference sources not found at $REF" >&2; exit 1; }

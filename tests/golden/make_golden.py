@@ -49,4 +49,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GSJ_REFERENCE_DIR", "")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_DIR (or set GSJ_REFERENCE_DIR)")
+    main(ref)

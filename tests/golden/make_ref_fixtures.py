@@ -17,7 +17,7 @@ DSSJ_out.txt, main.cu:544-565).  For every configuration it
   4. compares the per-point lists with the oracle under each candidate
      arithmetic model and records which model reproduces the reference.
 
-    python tests/golden/make_ref_fixtures.py --out gpurun_out/ref_pins.json
+    python tests/golden/make_ref_fixtures.py [--out tests/golden/ref_pins.json]
 """
 from __future__ import annotations
 
@@ -127,7 +127,7 @@ def main():
     from oracle import pyoracle as O
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "ref_pins.json"))
+    ap.add_argument("--out", default=os.path.join(HERE, "ref_pins.json"))
     ap.add_argument("--only", default="")
     ap.add_argument("--test-dat", default=os.path.join(HERE, "test_dat_f32.npy"))
     a = ap.parse_args()
