@@ -20,6 +20,7 @@ GSJ_FLAG_SORT_LISTS = 0x1
 GSJ_FLAG_QUIET = 0x2
 GSJ_FLAG_NO_UNICOMP = 0x4
 GSJ_FLAG_PLAIN = 0x8
+GSJ_FLAG_EXACT_SIZE = 0x10
 
 # Every symbol declared in include/gpuselfjoin.h.
 EXPORTED_SYMBOLS = (
@@ -64,6 +65,7 @@ class GsjStats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint64),
         ("join_path", ctypes.c_uint64),
         ("screen_rechecks", ctypes.c_uint64),
+        ("reruns", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

@@ -301,6 +301,26 @@ int d2h_small(gsj_context* c, X* dst, const X* src, size_t count) {
     return GSJ_OK;
 }
 
+// Entries a block-reserving pass may take for `real` entries: each warp
+// reserves blocks of kScreenBlockSlack entries and abandons its block (padding
+// the tail) when the next chunk of at most `max_chunk` entries does not fit,
+// so every abandoned block holds at least kScreenBlockSlack - (max_chunk - 1)
+// real entries; each of the `warps` warps may end with one partly filled block.
+uint64_t reserve_bound(uint64_t real, uint64_t warps, uint32_t max_chunk) {
+    const uint64_t per = kScreenBlockSlack - (max_chunk - 1u);
+    return ((real + per - 1u) / per + warps) * kScreenBlockSlack;
+}
+
+// Capacity of attempt `attempt` of a block-reserving pass: the estimate first;
+// after a short buffer the previous pass's own reservation `used` with room
+// for a different block-filling order; then the proven bound.  The first pass
+// runs with no buffer at all under GSJ_FLAG_EXACT_SIZE.
+uint64_t retry_cap(int attempt, uint64_t estimate, uint64_t used, uint64_t bound) {
+    if (attempt == 0) return estimate;
+    if (attempt == 1) return std::min(bound, used + used / 8u + (1u << 16));
+    return bound;
+}
+
 int validate(gsj_context* c, const gsj_config& cfg, uint64_t N) {
     if (cfg.dim == 0) return fail(c, GSJ_ERR_INVALID, "dim must be >= 1");
     if (cfg.dim > 4096) return fail(c, GSJ_ERR_INVALID, "dim above 4096 is not supported");
@@ -372,8 +392,8 @@ int pairs_to_csr(gsj_context* c, unsigned long long* pairs, uint64_t nsort, uint
 // the buffer; a short buffer is re-sized exactly and the pass repeated), then
 // the keys are sorted into the table.
 template <typename T>
-int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model, bool rows, uint32_t* counts,
-              uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
+int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model, bool rows, bool exact_size,
+              uint32_t* counts, uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
     constexpr uint32_t kSampleStride = 64;
     gsj_stats& S = c->stats;
     cudaStream_t st = c->st;
@@ -385,8 +405,10 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
     o.rechecks = cursor + 1; // keys emitted (exact)
     o.shift = shift;
     unsigned long long* cand = reinterpret_cast<unsigned long long*>(a.work_counter + 2);
-    // entries the warps may leave unused at the end: one block per resident warp
-    const uint64_t slack = (uint64_t)c->num_sms * 64u * kScreenBlockSlack;
+    // a warp appends at most 64 keys at once (32 hits and their reverse keys);
+    // at most 64 warps per SM are resident
+    const uint64_t warps = (uint64_t)c->num_sms * 64u;
+    const uint64_t slack = warps * kScreenBlockSlack;
     auto reset = [&]() -> int {
         GSJ_CUDA(c, cudaMemsetAsync(a.work_counter, 0, 4 * sizeof(uint32_t), st));
         GSJ_CUDA(c, cudaMemsetAsync(cursor, 0, 2 * sizeof(unsigned long long), st));
@@ -402,11 +424,13 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
     unsigned long long sampled = 0;
     GSJ_TRY(d2h_small(c, &sampled, o.rechecks, 1));
     const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
-    uint64_t cap = (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
+    const uint64_t estimate = exact_size ? 0u : (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
+    uint64_t cap = estimate;
     unsigned long long* pairs = nullptr;
     unsigned long long used = 0, R = 0;
-    for (int attempt = 0; attempt < 2; attempt++) {
-        GSJ_TRY(dev_get(c, c->pairs, cap, &pairs));
+    for (int attempt = 0; attempt < 3; attempt++) {
+        cap = retry_cap(attempt, estimate, used, reserve_bound(R, warps, 64u));
+        GSJ_TRY(dev_get(c, c->pairs, cap ? cap : 1, &pairs));
         GSJ_TRY(reset());
         o.emit = true;
         o.stride = 1;
@@ -417,8 +441,8 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
         GSJ_TRY(d2h_small(c, &used, cursor, 1));
         GSJ_TRY(d2h_small(c, &R, o.rechecks, 1));
         if (used <= cap) break;
-        if (attempt == 1) return fail(c, GSJ_ERR_STATE, "warp join: pair count changed between two passes");
-        cap = R + slack;
+        if (attempt == 2) return fail(c, GSJ_ERR_STATE, "warp join: pair buffer short at its proven bound");
+        c->stats.reruns++;
     }
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
     GSJ_TRY(pairs_to_csr(c, pairs, used, R, shift, N, counts, offsets, cand));
@@ -433,7 +457,7 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
 // data).  A sampling pass over every kSampleStride-th item sizes the pair
 // buffer; the full pass counts every pair even past the buffer, so a short
 // buffer is re-sized to the exact count and the pass repeated.
-int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int model, bool screen,
+int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int model, bool screen, bool exact_size,
               uint32_t* counts, uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
     constexpr uint32_t kSampleStride = 64;
     gsj_stats& S = c->stats;
@@ -445,8 +469,11 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
     o.cursor = cursor;
     o.shift = shift;
     o.rechecks = cursor + 1;  // the screen's exact count of undecided pairs
-    // entries the screen's consumer warps may leave unused: one block per warp
-    const uint64_t slack = screen ? (uint64_t)c->num_sms * 2u * 8u * kScreenBlockSlack : 0u;
+    // the screen's consumer warps reserve blocks (a warp appends at most
+    // 32 x 16 undecided pairs at once; at most 64 warps per SM are resident);
+    // the tile join appends exactly
+    const uint64_t warps = (uint64_t)c->num_sms * 64u;
+    const uint64_t slack = screen ? warps * kScreenBlockSlack : 0u;
     unsigned long long* cand = reinterpret_cast<unsigned long long*>(a.work_counter + 2);
     a.err_flag = a.work_counter + 1;
     ScreenConst sc = make_screen_const(a.n, a.thr);
@@ -490,13 +517,15 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         if (err) return fail(c, GSJ_ERR_CUDA, "tile join: tensor-core wait timed out");
     }
     const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
-    uint64_t cap = (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
-    // ---- full pass (repeated once with the exact size if the buffer was short):
+    const uint64_t estimate = exact_size ? 0u : (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
+    uint64_t cap = estimate;
+    // ---- full pass (repeated with a larger buffer if the buffer was short):
     // the tile join's hits, or the screen's undecided pairs
     unsigned long long *list = nullptr, *pairs = nullptr;
-    unsigned long long U = 0, R = 0, nlist = 0;
-    for (int attempt = 0; attempt < 2; attempt++) {
-        GSJ_TRY(dev_get(c, screen ? c->unc : c->pairs, cap, &list));
+    unsigned long long U = 0, R = 0, nlist = 0, used = 0;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        cap = retry_cap(attempt, estimate, used, screen ? reserve_bound(U, warps, 512u) : U);
+        GSJ_TRY(dev_get(c, screen ? c->unc : c->pairs, cap ? cap : 1, &list));
         GSJ_TRY(reset());
         o.emit = true;
         o.stride = 1;
@@ -504,7 +533,7 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         o.cap = cap;
         S.kernel_launches += 1;
         GSJ_CUDA(c, launch(ni));
-        unsigned long long used = 0;  // entries written (pairs, or reserved undecided blocks)
+        // entries written (pairs), or reserved (undecided blocks)
         GSJ_TRY(d2h_small(c, &used, cursor, 1));
         U = used;
         if (screen) GSJ_TRY(d2h_small(c, &U, o.rechecks, 1));
@@ -515,8 +544,8 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
             nlist = used;
             break;
         }
-        if (attempt == 1) return fail(c, GSJ_ERR_STATE, "tile join: pair count changed between two passes");
-        cap = U + slack;
+        if (attempt == 2) return fail(c, GSJ_ERR_STATE, "tile join: pair buffer short at its proven bound");
+        c->stats.reruns++;
     }
     if (screen) {
         // exact check of the undecided pairs; each yields at most one pair, two with unicomp
@@ -851,16 +880,17 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.rev_cnt = rev;
     a.cand_cnt = cand;
     const bool stamp = cfg.stamp != 0 && !(cfg.flags & GSJ_FLAG_NO_UNICOMP);
+    const bool exact_size = (cfg.flags & GSJ_FLAG_EXACT_SIZE) != 0;
     if constexpr (std::is_same<T, float>::value) {
         if (tile) {
             unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
-            return tile_join(c, a, N, stamp, model, screen, counts, offsets, cursor, t_join, t_start);
+            return tile_join(c, a, N, stamp, model, screen, exact_size, counts, offsets, cursor, t_join, t_start);
         }
     }
     // Every other grid except the thread-per-query rows: one emit pass + pair sort.
     if (!tpq) {
         unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
-        return emit_join<T>(c, a, N, stamp, model, rows, counts, offsets, cursor, t_join, t_start);
+        return emit_join<T>(c, a, N, stamp, model, rows, exact_size, counts, offsets, cursor, t_join, t_start);
     }
     // Dense low-dimensional grids (the thread-per-query rows): the distance
     // work is cheap and the cells too small for per-cell warp work, so one

@@ -128,9 +128,11 @@ cudaError_t launch_screen_prep(const float* pts, uint32_t N, uint32_t n, uint32_
 bool screen_supported(uint32_t n, uint32_t npad, uint32_t k, int model, uint32_t ilp, float thr);
 ScreenConst make_screen_const(uint32_t n, float thr);
 // Screen pass: the undecided pairs, packed as (query slot | cross << 31) << 32
-// | candidate slot, go to o.pairs in blocks that consumer warps reserve on
-// o.cursor (kScreenBlockSlack entries per warp at most stay unused, filled
-// with kUndecidedPad); o.rechecks receives their exact number.
+// | candidate slot, go to o.pairs in blocks of kScreenBlockSlack entries that
+// consumer warps reserve on o.cursor; a warp abandons its block when its next
+// chunk (up to 512 pairs) does not fit, padding the tail with kUndecidedPad,
+// so up to 511 entries of every block and most of each warp's last block can
+// stay unused; o.rechecks receives the exact number of undecided pairs.
 constexpr unsigned long long kUndecidedPad = ~0ull;
 constexpr uint64_t kScreenBlockSlack = 1024;
 cudaError_t launch_tile_screen(const JoinArgs<float>& a, const TileOut& o, const ScreenConst& sc, bool stamp,

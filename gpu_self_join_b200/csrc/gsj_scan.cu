@@ -151,8 +151,11 @@ extern "C" int gsj_list_offsets_noalloc(const uint32_t* d_counts, uint64_t n, ui
                                                  std::to_string(kNoAllocMaxCounts));
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return report_error(GSJ_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return report_error(GSJ_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices)
+        return report_error(GSJ_ERR_INVALID, "gsj_list_offsets_noalloc: device ordinal " + std::to_string(dev) +
+                                                 " beyond the " + std::to_string(kMaxDevices) +
+                                                 " devices whose scratch address is cached");
     void* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);

@@ -33,6 +33,7 @@ class JoinConfig:
     sort_lists: bool = False  # sort each neighbour list ascending
     no_unicomp: bool = False  # full-neighbourhood traversal even with stamp (same pair set)
     plain: bool = False       # no tensor-core screen (every pair in exact FP32; same pair set)
+    exact_size: bool = False  # pair buffers sized by a counting pass, not an estimate (same pair set)
 
 
 class SelfJoin:
@@ -73,7 +74,8 @@ class SelfJoin:
         c.query_reorder = int(cfg.query_reorder)
         c.device = self.device
         c.flags = (N.GSJ_FLAG_QUIET | (N.GSJ_FLAG_SORT_LISTS if cfg.sort_lists else 0)
-                   | (N.GSJ_FLAG_NO_UNICOMP if cfg.no_unicomp else 0) | (N.GSJ_FLAG_PLAIN if cfg.plain else 0))
+                   | (N.GSJ_FLAG_NO_UNICOMP if cfg.no_unicomp else 0) | (N.GSJ_FLAG_PLAIN if cfg.plain else 0)
+                   | (N.GSJ_FLAG_EXACT_SIZE if cfg.exact_size else 0))
         return c
 
     def run(self, points, eps: float, config: JoinConfig | None = None, **kw) -> dict:

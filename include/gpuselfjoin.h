@@ -54,6 +54,11 @@ extern "C" {
                                      (same pair set, different work split)   */
 #define GSJ_FLAG_PLAIN      0x8u  /* no tensor-core screen: every candidate pair
                                      is evaluated with the exact FP32 arithmetic */
+#define GSJ_FLAG_EXACT_SIZE 0x10u /* size the pair buffers of the warp, tile and
+                                     screen paths without an estimate: the first
+                                     pass only counts, the pass is repeated into a
+                                     buffer of the counted size (the re-run path
+                                     that a short estimate takes)              */
 
 /*
  * Run-time configuration.  Field names follow params.h of the reference
@@ -95,6 +100,8 @@ typedef struct gsj_stats {
     uint64_t join_path;       /* GSJ_PATH_* taken by the last join              */
     uint64_t screen_rechecks; /* GSJ_PATH_SCREEN: pairs the BF16 screen could not
                                  reject, evaluated exactly (0 on other paths)   */
+    uint64_t reruns;          /* passes repeated because a buffer sized from the
+                                 estimate was short (the output is unchanged)  */
 } gsj_stats;
 
 /* Join paths (gsj_stats.join_path). */
@@ -187,7 +194,9 @@ GSJ_API int gsj_bruteforce_count(gsj_context* ctx, const void* data, uint64_t nu
  * cudaStream_t, NULL for the legacy default stream) and the call returns
  * without waiting for it.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) and caches it; make that first call
- * before any stream capture.  All calls share the one array, which keeps the
+ * before any stream capture.  The cached address belongs to the device's
+ * context of that first call: after a cudaDeviceReset of the device, use the
+ * entry point only from a new process.  All calls share the one array, which keeps the
  * last call's contents (nothing in it needs to start at zero): calls that
  * overlap on the GPU, e.g. on two streams at once, race and must be ordered by
  * the caller.

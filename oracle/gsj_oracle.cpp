@@ -707,3 +707,68 @@ extern "C" int orc_join_sample_f32(const float* p, uint64_t N, uint32_t n, float
                                    const uint32_t* q, uint64_t nq, uint64_t* total, double* si, double* sq) {
     return join_sample<float>(p, N, n, eps, *cfg, q, nq, total, si, sq);
 }
+
+// ---------------------------------------------------------------- sample lists
+// Sorted neighbour lists of a query sample (the full-size workloads' parity
+// tests): the index over all N points, then the full enumeration of `join`
+// (kernel.cu:292-302) for the listed queries only.  counts[i] receives query
+// q[i]'s list length and *total their sum; when *total <= cap the lists are
+// written to `lists`, query after query, each ascending.  The model may be
+// any of the decision models (MODEL_FP64 for the double-precision decision).
+namespace {
+template <typename T>
+int sample_lists(const T* pts, uint64_t N, uint32_t n, T eps, const orc_cfg& cfg, const uint32_t* q, uint64_t nq,
+                 uint32_t* counts, uint32_t* lists, uint64_t cap, uint64_t* total) {
+    if (cfg.k == 0 || cfg.k > n || cfg.k > 64 || cfg.ilp > 64) return -1;
+    for (uint64_t i = 0; i < nq; i++)
+        if (q[i] >= N) return -2;
+    Prepared<T> P;
+    prepare<T>(pts, N, n, eps, cfg, P);
+    const Grid<T>& g = P.g;
+    const T* D = P.data.data();
+    std::vector<std::vector<uint32_t>> out(nq);
+    int nth = cfg.nthreads ? (int)cfg.nthreads : 0;
+#ifdef _OPENMP
+    if (nth <= 0) nth = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nth)
+#endif
+    for (int64_t i = 0; i < (int64_t)nq; i++) {
+        const T* p = D + (uint64_t)q[i] * n;
+        uint32_t own[64], rmin[64], rmax[64];
+        query_ranges<T>(p, eps, g, own, rmin, rmax);
+        std::vector<uint32_t>& v = out[i];
+        auto visit = [&](const uint32_t* idx, bool) {
+            int64_t ci = find_cell(g.cellIds, linear_id(idx, g.nCells.data(), g.k));
+            if (ci < 0) return;
+            for (uint32_t s = g.cellBegin[ci]; s < g.cellEnd[ci]; s++)
+                if (within<T>(p, D + (uint64_t)g.lookup[s] * n, n, eps, cfg)) v.push_back(g.lookup[s]);
+        };
+        for_each_cell(g.k, own, rmin, rmax, false, visit);
+        std::sort(v.begin(), v.end());
+    }
+    uint64_t tot = 0;
+    for (uint64_t i = 0; i < nq; i++) {
+        counts[i] = (uint32_t)out[i].size();
+        tot += out[i].size();
+    }
+    *total = tot;
+    if (lists && tot <= cap) {
+        uint64_t o = 0;
+        for (uint64_t i = 0; i < nq; i++) {
+            std::copy(out[i].begin(), out[i].end(), lists + o);
+            o += out[i].size();
+        }
+    }
+    return 0;
+}
+}  // namespace
+extern "C" int orc_sample_lists_f32(const float* p, uint64_t N, uint32_t n, float eps, const orc_cfg* cfg,
+                                    const uint32_t* q, uint64_t nq, uint32_t* counts, uint32_t* lists, uint64_t cap,
+                                    uint64_t* total) {
+    return sample_lists<float>(p, N, n, eps, *cfg, q, nq, counts, lists, cap, total);
+}
+extern "C" int orc_sample_lists_f64(const double* p, uint64_t N, uint32_t n, double eps, const orc_cfg* cfg,
+                                    const uint32_t* q, uint64_t nq, uint32_t* counts, uint32_t* lists, uint64_t cap,
+                                    uint64_t* total) {
+    return sample_lists<double>(p, N, n, eps, *cfg, q, nq, counts, lists, cap, total);
+}

@@ -102,6 +102,8 @@ def lib():
             getattr(_lib, f"orc_import_text_{sfx}").argtypes = [ctypes.c_char_p, u32, P, u64]
             getattr(_lib, f"orc_import_text_{sfx}").restype = i64
         _lib.orc_join_sample_f32.argtypes = [P, u64, u32, ctypes.c_float, P, P, u64, P, P, P]
+        _lib.orc_sample_lists_f32.argtypes = [P, u64, u32, ctypes.c_float, P, P, u64, P, P, u64, P]
+        _lib.orc_sample_lists_f64.argtypes = [P, u64, u32, ctypes.c_double, P, P, u64, P, P, u64, P]
         _lib.orc_ref_batch_plan_f32.argtypes = [P, u64, u32, ctypes.c_float, P, P, P, u32,
                                                 ctypes.c_double, P, P, P, P]
     return _lib
@@ -240,3 +242,28 @@ def join_sample(points: np.ndarray, eps: float, cfg: OracleConfig, queries: np.n
     lib().orc_join_sample_f32(p.ctypes.data, N, n, eps, ctypes.byref(c), q.ctypes.data, q.size, ctypes.byref(tot),
                               ctypes.byref(si), ctypes.byref(sq))
     return int(tot.value), float(si.value), float(sq.value)
+
+
+def sample_lists(points: np.ndarray, eps: float, cfg: OracleConfig, queries: np.ndarray):
+    """Sorted neighbour lists of the listed queries (full enumeration, the
+    configured decision model): (counts uint32[nq], lists uint32[sum]), the
+    lists concatenated in the order of `queries`."""
+    p = _prep(points)
+    N, n = p.shape
+    q = np.ascontiguousarray(queries, dtype=np.uint32)
+    counts = np.zeros(q.size, dtype=np.uint32)
+    tot = ctypes.c_uint64()
+    c = cfg.c(p.dtype)
+    f = getattr(lib(), f"orc_sample_lists_{_sfx(p)}")
+    cap = max(1, 64 * q.size)
+    lists = np.zeros(cap, dtype=np.uint32)
+    rc = f(p.ctypes.data, N, n, eps, ctypes.byref(c), q.ctypes.data, q.size, counts.ctypes.data, lists.ctypes.data,
+           cap, ctypes.byref(tot))
+    if rc != 0:
+        raise ValueError(f"oracle rejected the configuration (rc={rc})")
+    if tot.value > cap:
+        cap = int(tot.value)
+        lists = np.zeros(cap, dtype=np.uint32)
+        f(p.ctypes.data, N, n, eps, ctypes.byref(c), q.ctypes.data, q.size, counts.ctypes.data, lists.ctypes.data,
+          cap, ctypes.byref(tot))
+    return counts, lists[: int(tot.value)]

@@ -68,7 +68,26 @@ def test_noalloc_offsets_match_join_twice():
             torch.cuda.synchronize()
             got = out.cpu().numpy().view(np.uint64)
             assert np.array_equal(got, ref)
+            # independent of the library's scan: the prefix of the host counts
+            want = np.concatenate([[0], np.cumsum(host_counts, dtype=np.uint64)]).astype(np.uint64)
+            assert np.array_equal(got, want)
             assert int(got[-1]) == int(host_counts.sum(dtype=np.uint64)) == sj.total_pairs()
+
+
+def test_noalloc_empty_input_writes_zero_total():
+    """n = 0: the single offset (the total) is zero, whatever the output held."""
+    import torch
+
+    from gpu_self_join_b200._native import lib
+
+    L = lib()
+    counts = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = torch.full((1,), 12345, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    rc = L.gsj_list_offsets_noalloc(ctypes.c_void_p(counts.data_ptr()), 0, ctypes.c_void_p(out.data_ptr()), None)
+    assert rc == 0, L.gsj_last_error(None)
+    torch.cuda.synchronize()
+    assert int(out.cpu()[0]) == 0
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
