@@ -29,15 +29,13 @@
 #include <type_traits>
 #include <vector>
 
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_run_length_encode.cuh>
-#include <cub/device/device_scan.cuh>
-#include <cub/device/device_segmented_sort.cuh>
 
 #include "../../include/gpuselfjoin.h"
 #include "gsj_common.cuh"
 #include "gsj_kernels.h"
+#include "gsj_place.h"
 #include "gsj_scan.h"
+#include "gsj_sort.h"
 
 // Build-time defaults, same macro names as the reference's params.h.
 #ifndef GPUNUMDIM
@@ -135,6 +133,13 @@ bool compareByDimVariance(const dim_reorder_sort<T>& a, const dim_reorder_sort<T
     return a.variance > b.variance;
 }
 
+// Scalars of a join in the context's `misc` buffer (at least 512 bytes):
+// min/max per indexed dim (2 kMaxK values of T), then 32-bit words: run count,
+// work counter, error flag, candidate counter (64-bit), pair cursors (2 x
+// 64-bit); the pair placement's error flag and long-list count at words
+// 4 kMaxK + 20 and + 24, the longest list at + 28 (bytes 240, 256 and 272).
+constexpr size_t kMiscWords = 128;
+
 uint32_t npad_of(uint32_t n, uint32_t tsize) {
     return n <= 2 ? n : ((n + (16u / tsize) - 1u) / (16u / tsize)) * (16u / tsize);
 }
@@ -149,10 +154,10 @@ struct gsj_context {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaEvent_t tev[6] = {};  // stage timing: index start/end, count start/end, fill start/end
     // device pool
-    Buf in, pts, ids, keys, keys2, vals, cell_key, runs, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
+    Buf in, pts, ids, keys, keys2, vals, cell_key, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
-        item_off, items, fwd, rev, counts, offsets, table, temp, scan_temp, misc, var, perm, minarr,
-        minmax_part, pairs, pairs2, srows, snorms, spartial, scentre, unc, table2, nbtab;
+        item_off, items, fwd, swords, counts, offsets, table, temp, scan_temp, misc, var, perm, minarr,
+        minmax_part, pairs, srows, snorms, spartial, scentre, unc, table2, nbtab, bitoff, hitbits, ptemp;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
     // last result
@@ -333,41 +338,59 @@ int validate(gsj_context* c, const gsj_config& cfg, uint64_t N) {
     return GSJ_OK;
 }
 
+// ------------------------------------------------------------------ lists ascending
+// Sorts every list of the table ascending (ids below N): a warp per short
+// list, a CTA per long one with a scratch copy of the table.
+int sort_table_lists(gsj_context* c, uint32_t* table, const uint64_t* offsets, uint64_t N, uint64_t R) {
+    gsj_stats& S = c->stats;
+    cudaStream_t st = c->st;
+    int nl = 0;
+    GSJ_CUDA(c, sort_short_lists(table, offsets, (uint32_t)N, c->num_sms, &nl, st));
+    void* temp = nullptr;
+    GSJ_TRY(dev_get(c, c->ptemp, place_temp_bytes(N), (unsigned char**)&temp));
+    uint32_t* d_nlong = reinterpret_cast<uint32_t*>(c->misc.p) + 4 * kMaxK + 24;
+    uint32_t nlong = 0;
+    GSJ_CUDA(c, find_long_lists(offsets, (uint32_t)N, temp, d_nlong, &nlong, &nl, st));
+    if (nlong) {
+        uint32_t* scratch = nullptr;
+        GSJ_TRY(dev_get(c, c->table2, R, &scratch));
+        uint32_t id_bits = 1;
+        while (id_bits < 32 && ((N - 1) >> id_bits)) id_bits++;
+        GSJ_CUDA(c, sort_long_lists(table, scratch, offsets, temp, nlong, id_bits, c->num_sms, &nl, st));
+    }
+    S.kernel_launches += (uint64_t)nl;
+    return GSJ_OK;
+}
+
 // ------------------------------------------------------------------ pair keys -> table
-// Sorts `nsort` packed (query id << shift | candidate id) keys on the device
-// (entries past the R real keys are pads, which sort last), writes the
-// neighbour table (low bits) and the list lengths and offsets, and fills the
+// Builds the neighbour table from `nkeys` packed (query id << shift |
+// candidate id) keys (entries equal to ~0 are unused block tails): list
+// lengths, offsets, placement, then every list sorted ascending.  Fills the
 // stage times and the result state.  cand: the device candidate counter.
-int pairs_to_csr(gsj_context* c, unsigned long long* pairs, uint64_t nsort, uint64_t R, uint32_t shift, uint64_t N,
+int pairs_to_csr(gsj_context* c, unsigned long long* pairs, uint64_t nkeys, uint64_t R, uint32_t shift, uint64_t N,
                  uint32_t* counts, uint64_t* offsets, const unsigned long long* cand) {
     gsj_stats& S = c->stats;
     cudaStream_t st = c->st;
     GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
-    unsigned long long* sorted = nullptr;
-    uint32_t* table = nullptr;
-    GSJ_TRY(dev_get(c, c->pairs2, nsort ? nsort : 1, &sorted));
+    uint32_t *table = nullptr, *cursor = nullptr;
     GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
-    GSJ_CUDA(c, cudaMemsetAsync(counts, 0, (N + 1) * sizeof(uint32_t), st));
-    if (R) {
-        // one bit above the keys, clear in every key and set in the pads
-        const int end_bit = (int)(2 * shift + 1);
-        size_t tb = 0;
-        void* temp = nullptr;
-        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(nullptr, tb, pairs, sorted, (uint64_t)nsort, 0, end_bit, st));
-        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-        GSJ_CUDA(c, cub::DeviceRadixSort::SortKeys(temp, tb, pairs, sorted, (uint64_t)nsort, 0, end_bit, st));
-        S.kernel_launches += (uint64_t)(end_bit + 7) / 8 + 2;
-        S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_pairs_to_table(sorted, R, shift, table, counts, c->num_sms, st));
-    }
-    void* stemp = nullptr;
-    GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
-    S.kernel_launches += 3;
-    GSJ_CUDA(c, scan_u32_u64(counts, offsets, N, stemp, st));
+    GSJ_TRY(dev_get(c, c->fwd, N, &cursor));
+    void* temp = nullptr;
+    GSJ_TRY(dev_get(c, c->ptemp, place_temp_bytes(N), (unsigned char**)&temp));
+    uint32_t* d_err = reinterpret_cast<uint32_t*>(c->misc.p) + 4 * kMaxK + 20;
+    GSJ_CUDA(c, cudaMemsetAsync(d_err, 0, sizeof(uint32_t), st));
+    int nl = 0;
+    GSJ_CUDA(c, place_pairs(pairs, nkeys, shift, (uint32_t)N, counts, offsets, table, R, cursor, d_err, temp,
+                            c->num_sms, &nl, st));
+    S.kernel_launches += (uint64_t)nl;
+    GSJ_TRY(sort_table_lists(c, table, offsets, N, R));
     GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
     uint64_t total = 0;
     GSJ_TRY(d2h_small(c, &total, offsets + N, 1));
     if (total != R) return fail(c, GSJ_ERR_STATE, "list lengths disagree with the pair count");
+    uint32_t err = 0;
+    GSJ_TRY(d2h_small(c, &err, d_err, 1));
+    if (err) return fail(c, GSJ_ERR_STATE, "pair placement left a list (internal error)");
     unsigned long long ncand = 0;
     GSJ_TRY(d2h_small(c, &ncand, cand, 1));
     {
@@ -640,7 +663,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     const uint32_t nparts = (uint32_t)std::min<uint64_t>((N + 255) / 256, (uint64_t)c->num_sms * 4);
     T *d_part = nullptr, *d_mm = nullptr;
     GSJ_TRY(dev_get(c, c->minmax_part, (size_t)nparts * 2 * k, &d_part));
-    GSJ_TRY(dev_get(c, c->misc, 2 * kMaxK + 16, &d_mm));
+    GSJ_TRY(dev_get(c, c->misc, kMiscWords, &d_mm));
     S.kernel_launches += 2;
     GSJ_CUDA(c, launch_minmax<T>(d_in, N, n, k, d_perm, d_part, nparts, d_mm, st));
     std::vector<T> mm(2 * k);
@@ -701,39 +724,55 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     GSJ_TRY(dev_get(c, c->minarr, k, &d_min));
     GSJ_CUDA(c, cudaMemcpyAsync(d_min, minArr.data(), k * sizeof(T), cudaMemcpyHostToDevice, st));
 
-    // ---- cell keys + radix sort (subsystem (a))
+    // ---- cell keys + radix sort (subsystem (a)): points ordered by cell, ties
+    // by point id (a stable sort of keys generated in point-id order)
     uint64_t *keys = nullptr, *keys2 = nullptr;
     uint32_t *vals = nullptr, *ids = nullptr;
     GSJ_TRY(dev_get(c, c->keys, N, &keys));
     GSJ_TRY(dev_get(c, c->keys2, N, &keys2));
     GSJ_TRY(dev_get(c, c->vals, N, &vals));
     GSJ_TRY(dev_get(c, c->ids, N, &ids));
-    S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_cell_keys<T>(d_in, N, n, d_perm, g, d_min, eps, keys, vals, st));
     int bits = 1;
     while (bits < 64 && (totalCells - 1) >> bits) bits++;
-    size_t tb = 0;
-    GSJ_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, vals, ids, (int)N, 0, bits, st));
+    const bool key32 = bits <= 32;
     void* temp = nullptr;
-    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-    GSJ_CUDA(c, cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, ids, (int)N, 0, bits, st));
+    GSJ_TRY(dev_get(c, c->temp, std::max(radix_sort_temp_bytes(N), runs_temp_bytes(N)), (unsigned char**)&temp));
+    bool in_alt = false;
+    int nl = 0;
+    S.kernel_launches += 1;
+    if (key32) {
+        uint32_t* k32 = reinterpret_cast<uint32_t*>(keys);
+        uint32_t* k32b = reinterpret_cast<uint32_t*>(keys2);
+        GSJ_CUDA(c, (launch_cell_keys<T, uint32_t>(d_in, N, n, d_perm, g, d_min, eps, k32, vals, st)));
+        GSJ_CUDA(c, radix_sort<uint32_t>(k32, k32b, vals, ids, N, 0, bits, temp, &in_alt, &nl, st));
+    } else {
+        GSJ_CUDA(c, (launch_cell_keys<T, uint64_t>(d_in, N, n, d_perm, g, d_min, eps, keys, vals, st)));
+        GSJ_CUDA(c, radix_sort<uint64_t>(keys, keys2, vals, ids, N, 0, bits, temp, &in_alt, &nl, st));
+    }
+    S.kernel_launches += (uint64_t)nl;
+    if (!in_alt) {
+        // an even number of passes (or none) leaves the result in the first buffers
+        std::swap(c->keys, c->keys2);
+        std::swap(c->vals, c->ids);
+        std::swap(keys, keys2);
+        std::swap(vals, ids);
+    }
 
-    // ---- runs of equal keys = non-empty cells
+    // ---- runs of equal keys = non-empty cells: cell_key[M], cell_start[M+1]
     uint64_t* cell_key = nullptr;
-    uint32_t *runs = nullptr, *cell_start = nullptr, *d_nruns = nullptr;
+    uint32_t *cell_start = nullptr, *d_nruns = nullptr;
     GSJ_TRY(dev_get(c, c->cell_key, N, &cell_key));
-    GSJ_TRY(dev_get(c, c->runs, N + 1, &runs));
     GSJ_TRY(dev_get(c, c->cell_start, N + 1, &cell_start));
     d_nruns = reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK);
-    GSJ_CUDA(c, cub::DeviceRunLengthEncode::Encode(nullptr, tb, keys2, cell_key, runs, d_nruns, (int)N, st));
-    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-    GSJ_CUDA(c, cub::DeviceRunLengthEncode::Encode(temp, tb, keys2, cell_key, runs, d_nruns, (int)N, st));
+    S.kernel_launches += 5;
+    if (key32)
+        GSJ_CUDA(c, run_length<uint32_t>(reinterpret_cast<const uint32_t*>(keys2), N, cell_key, cell_start, d_nruns,
+                                         temp, st));
+    else
+        GSJ_CUDA(c, run_length<uint64_t>(keys2, N, cell_key, cell_start, d_nruns, temp, st));
     uint32_t M = 0;
     GSJ_TRY(d2h_small(c, &M, d_nruns, 1));
     S.nonempty_cells = M;
-    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tb, runs, cell_start, (int)M, st));
-    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(temp, tb, runs, cell_start, (int)M, st));
 
     // ---- points in cell order
     T* pts = nullptr;
@@ -762,12 +801,13 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_TRY(dev_get(c, c->hvals, hcap, &hvals));
         GSJ_CUDA(c, cudaMemsetAsync(hkeys, 0xff, hcap * sizeof(unsigned long long), st));
     }
-    S.kernel_launches += 2;
-    GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, runs, M, (uint32_t)N, dcnt, hkeys, hvals, hmask, st));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, M, dcnt, hkeys, hvals, hmask, st));
     if (dense) {
-        GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tb, dcnt, ds, (int)(totalCells + 1), st));
-        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-        GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(temp, tb, dcnt, ds, (int)(totalCells + 1), st));
+        // the slot-prefix table: ds[L] = points in cells below L (ds[totalCells] = N)
+        GSJ_TRY(dev_get(c, c->temp, scan_u32_u64_temp_bytes(totalCells), (unsigned char**)&temp));
+        S.kernel_launches += 3;
+        GSJ_CUDA(c, scan_u32_u32(dcnt, ds, totalCells, temp, st));
     }
     // Dense low-dimensional grids use the row-range traversal driven by a
     // per-cell plan of neighbour-row slot ranges.
@@ -782,11 +822,20 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_CUDA(c, launch_cell_plan(cell_key, M, g, ds, plan, plan_par, st));
     }
     uint32_t* slot_cell = nullptr;
+    uint64_t* bitoff = nullptr;
     const bool tpq = rows && cfg.ilp == 0 && n <= 4;
     if (tpq) {
+        // slot -> cell, and the hit-mask layout: slot s's query owns words
+        // [bitoff[s], bitoff[s+1]) of the count pass's bit masks
+        uint32_t* swords = nullptr;
+        const uint32_t nrows = k == 1 ? 1u : (k == 2 ? 3u : 9u);
         GSJ_TRY(dev_get(c, c->slot_cell, N, &slot_cell));
-        S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_slot_cell(cell_start, M, slot_cell, st));
+        GSJ_TRY(dev_get(c, c->swords, N, &swords));
+        GSJ_TRY(dev_get(c, c->bitoff, N + 1, &bitoff));
+        GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&temp));
+        S.kernel_launches += 4;
+        GSJ_CUDA(c, launch_slot_cell(cell_start, M, plan, nrows, slot_cell, swords, st));
+        GSJ_CUDA(c, scan_u32_u64(swords, bitoff, N, temp, st));
     }
 
     // High-dimensional float data with populated cells (at least 8 points per
@@ -813,26 +862,29 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         sizes2 = sizes + M;
         GSJ_TRY(dev_get(c, c->order, 2 * (size_t)M, &order));
         iota = order + M;
+        // stable descending sort by cell size (ties keep ascending cell order):
+        // an ascending sort of the complemented sizes
+        S.kernel_launches += 2;
+        GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, sizes, st));
+        GSJ_CUDA(c, launch_iota(iota, M, st));
+        GSJ_TRY(dev_get(c, c->temp, radix_sort_temp_bytes(M), (unsigned char**)&temp));
+        bool alt = false;
+        int nl2 = 0;
+        GSJ_CUDA(c, radix_sort<uint32_t>(sizes, sizes2, iota, order, M, 0, 32, temp, &alt, &nl2, st));
+        S.kernel_launches += (uint64_t)nl2;
+        if (!alt) {
+            // the sorted cell indices are in iota (order + M): move them to order[0, M)
+            GSJ_CUDA(c, cudaMemcpyAsync(order, iota, (size_t)M * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+        }
         S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, sizes, st));
-        S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_iota(iota, M, st));
-        // stable descending sort by cell size: ties keep ascending cell order
-        GSJ_CUDA(c, cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, sizes, sizes2, iota, order, (int)M, 0, 32,
-                                                              st));
-        GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-        GSJ_CUDA(c, cub::DeviceRadixSort::SortPairsDescending(temp, tb, sizes, sizes2, iota, order, (int)M, 0, 32,
-                                                              st));
-        S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_item_counts(cell_start, order, M, qchunk, nchunks, nullptr, st));
+        GSJ_CUDA(c, launch_item_counts(cell_start, order, M, qchunk, nchunks, nullptr, st));
     } else {
         S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, nullptr, st));
+        GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, nullptr, st));
     }
-    GSJ_CUDA(c, cudaMemsetAsync(nchunks + M, 0, sizeof(uint32_t), st));
-    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tb, nchunks, item_off, (int)M + 1, st));
-    GSJ_TRY(dev_get(c, c->temp, tb, (unsigned char**)&temp));
-    GSJ_CUDA(c, cub::DeviceScan::ExclusiveSum(temp, tb, nchunks, item_off, (int)M + 1, st));
+    GSJ_TRY(dev_get(c, c->temp, scan_u32_u64_temp_bytes(M), (unsigned char**)&temp));
+    S.kernel_launches += 3;
+    GSJ_CUDA(c, scan_u32_u32(nchunks, item_off, M, temp, st));
     uint32_t num_items = 0;
     GSJ_TRY(d2h_small(c, &num_items, item_off + M, 1));
     S.work_items = num_items;
@@ -845,13 +897,11 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     const double t_join = now_ms();
     S.ms_index = t_join - t_index;
 
-    // ---- join arguments (every path); per-slot counts for the ROWS count pass
-    uint32_t *fwd = nullptr, *rev = nullptr;
-    GSJ_TRY(dev_get(c, c->fwd, N, &fwd));
-    GSJ_TRY(dev_get(c, c->rev, N, &rev));
+    // ---- join arguments (every path); per-slot list lengths of the ROWS path
+    uint32_t* fwd = nullptr;
+    if (tpq) GSJ_TRY(dev_get(c, c->fwd, N, &fwd));
     uint32_t* ctr = reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK) + 2;  // work counter
     unsigned long long* cand = reinterpret_cast<unsigned long long*>(reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK) + 4);
-    GSJ_CUDA(c, cudaMemsetAsync(rev, 0, N * sizeof(uint32_t), st));
     GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, 4 * sizeof(uint32_t), st));
     JoinArgs<T> a{};
     a.pts = pts;
@@ -877,7 +927,6 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.eps = eps;
     for (uint32_t j = 0; j < k; j++) a.minv[j] = minArr[j];
     a.fwd_cnt = fwd;
-    a.rev_cnt = rev;
     a.cand_cnt = cand;
     const bool stamp = cfg.stamp != 0 && !(cfg.flags & GSJ_FLAG_NO_UNICOMP);
     const bool exact_size = (cfg.flags & GSJ_FLAG_EXACT_SIZE) != 0;
@@ -892,18 +941,22 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
         return emit_join<T>(c, a, N, stamp, model, rows, exact_size, counts, offsets, cursor, t_join, t_start);
     }
-    // Dense low-dimensional grids (the thread-per-query rows): the distance
-    // work is cheap and the cells too small for per-cell warp work, so one
-    // thread per query counts its full neighbourhood, and the fill pass writes
-    // every list forward only (contiguous, deterministic).
+    // Dense low-dimensional grids (the ROWS path): the distance work is cheap
+    // and the cells too small for per-cell warp work, so one thread per query
+    // evaluates its full neighbourhood once, recording the decisions as a bit
+    // mask; the fill pass replays the masks into the table.
+    uint32_t* hitbits = nullptr;
+    {
+        uint64_t nwords = 0;
+        GSJ_TRY(d2h_small(c, &nwords, bitoff + N, 1));
+        GSJ_TRY(dev_get(c, c->hitbits, nwords ? nwords : 1, &hitbits));
+    }
     GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
     S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_count_tpq<T>(a, slot_cell, c->num_sms, st));
+    GSJ_CUDA(c, launch_rows_count<T>(a, slot_cell, bitoff, hitbits, counts, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
 
-    // ---- list lengths and offsets
-    S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_sum_counts(fwd, rev, ids, N, counts, st));
+    // ---- list offsets (counts are by point id)
     void* stemp = nullptr;
     GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
     S.kernel_launches += 3;
@@ -924,9 +977,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.err_flag = ctr + 1;  // zeroed with the counters before the count pass
     GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
     S.kernel_launches += 1;
-    // a warp per 32 consecutive query slots (consecutive queries share their
-    // cell's candidate tiles)
-    GSJ_CUDA(c, launch_fill_q32<T>(a, slot_cell, c->num_sms, st));
+    GSJ_CUDA(c, launch_rows_fill<T>(a, slot_cell, bitoff, hitbits, nullptr, (uint32_t)N, 0, c->num_sms, st));
     GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
     GSJ_CUDA(c, cudaStreamSynchronize(st));
     {
@@ -940,23 +991,11 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     }
     uint32_t errflag = 0;
     GSJ_TRY(d2h_small(c, &errflag, ctr + 1, 1));
-    if (errflag) return fail(c, GSJ_ERR_STATE, "fill pass disagreed with the count pass (table bound reached)");
+    if (errflag) return fail(c, GSJ_ERR_STATE, "fill pass: a list would leave the table (internal error)");
     if ((cfg.flags & GSJ_FLAG_SORT_LISTS) && R > 1) {
-        // every list ascending: a segmented sort of the table over the list offsets
-        if (R > 0x7fffffffull || N > 0x7fffffffull)
-            return fail(c, GSJ_ERR_INVALID, "GSJ_FLAG_SORT_LISTS needs fewer than 2^31 result pairs on this path");
-        uint32_t* sorted = nullptr;
-        GSJ_TRY(dev_get(c, c->table2, R, &sorted));
-        size_t tb2 = 0;
-        GSJ_CUDA(c, cub::DeviceSegmentedSort::SortKeys(nullptr, tb2, table, sorted, (int)R, (int)N, offsets,
-                                                       offsets + 1, st));
-        void* temp2 = nullptr;
-        GSJ_TRY(dev_get(c, c->temp, tb2, (unsigned char**)&temp2));
-        GSJ_CUDA(c, cub::DeviceSegmentedSort::SortKeys(temp2, tb2, table, sorted, (int)R, (int)N, offsets,
-                                                       offsets + 1, st));
-        S.kernel_launches += 4;
+        // every list ascending
+        GSJ_TRY(sort_table_lists(c, table, offsets, N, R));
         GSJ_CUDA(c, cudaStreamSynchronize(st));
-        std::swap(c->table, c->table2);
     }
     S.ms_join = now_ms() - t_join;
     S.total_pairs = R;
@@ -1044,13 +1083,13 @@ int gsj_destroy(gsj_context* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamSynchronize(c->st2);
     Buf* bufs[] = {&c->in,       &c->pts,   &c->ids,    &c->keys,      &c->keys2,   &c->vals,      &c->cell_key,
-                   &c->runs,     &c->cell_start, &c->dense, &c->dcnt, &c->plan, &c->plan_par, &c->slot_cell, &c->hkeys,
+                   &c->cell_start, &c->dense, &c->dcnt, &c->plan, &c->plan_par, &c->slot_cell, &c->hkeys,
                    &c->hvals,
                    &c->order,    &c->sizes,
-                   &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->rev,     &c->counts,    &c->offsets,
+                   &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->swords,     &c->counts,    &c->offsets,
                    &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
-                   &c->minarr,   &c->minmax_part, &c->pairs, &c->pairs2, &c->srows, &c->snorms,
-                   &c->spartial, &c->scentre, &c->unc, &c->table2, &c->nbtab};
+                   &c->minarr,   &c->minmax_part, &c->pairs, &c->srows, &c->snorms,
+                   &c->spartial, &c->scentre, &c->unc, &c->table2, &c->nbtab, &c->bitoff, &c->hitbits, &c->ptemp};
     for (Buf* b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})
@@ -1102,7 +1141,7 @@ int gsj_bruteforce_count(gsj_context* c, const void* data, uint64_t num_points, 
     uint32_t* d_counts = nullptr;
     unsigned long long* d_total = nullptr;
     GSJ_TRY(dev_get(c, c->counts, (size_t)N + 1, &d_counts));
-    GSJ_TRY(dev_get(c, c->misc, 2 * kMaxK + 16, reinterpret_cast<double**>(&d_total)));
+    GSJ_TRY(dev_get(c, c->misc, kMiscWords, reinterpret_cast<double**>(&d_total)));
     GSJ_CUDA(c, cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), st));
     if (cfg->dtype == GSJ_FLOAT32) {
         const float e = (float)eps;

@@ -48,11 +48,10 @@ struct JoinArgs {
     T thr;                        // s <= thr  <=>  sqrt(s) <= eps
     T eps;                        // epsilon in T (cell formula)
     T minv[kMaxK];                // minArr (grid origin per indexed dim)
-    // counts (thread-per-query rows; the emit join adds to cand_cnt only)
-    uint32_t* fwd_cnt;            // [N] by slot
-    uint32_t* rev_cnt;            // [N] by slot (unicomp reverse hits)
+    // counts (ROWS path; the other paths add to cand_cnt only)
+    uint32_t* fwd_cnt;            // [N] list length by slot
     unsigned long long* cand_cnt; // candidate evaluations
-    // fill pass (thread-per-query rows)
+    // fill pass (ROWS path)
     const uint64_t* offsets;      // [N+1] by original id
     uint32_t* table;              // [R]
     unsigned long long table_cap; // R: writes at or beyond it are dropped and flagged

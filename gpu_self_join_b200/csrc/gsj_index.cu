@@ -130,10 +130,10 @@ __global__ void k_minmax_final(const T* __restrict__ part, uint32_t nparts, uint
 // ------------------------------------------------------------ cell keys
 // Cell coordinate (x - minArr)/eps truncated to unsigned (main.cu:713,744 and
 // kernel.cu:184 compute it identically), linear id with dim 0 fastest.
-template <typename T>
+template <typename T, typename K>
 __global__ void k_cell_keys(const T* __restrict__ in, uint64_t N, uint32_t n, const uint32_t* __restrict__ perm,
                             GridGeom g, const T* __restrict__ minArr, T eps,
-                            uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+                            K* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (i >= N) return;
     uint64_t key = 0;
@@ -144,7 +144,7 @@ __global__ void k_cell_keys(const T* __restrict__ in, uint64_t N, uint32_t n, co
             const uint32_t c = FP<T>::to_uint_rz(FP<T>::div(FP<T>::sub(x, minArr[j]), eps));
             key += (uint64_t)c * g.mult[j];
         }
-    keys[i] = key;
+    keys[i] = (K)key;
     vals[i] = (uint32_t)i;
 }
 
@@ -161,16 +161,12 @@ __global__ void k_gather_points(const T* __restrict__ in, uint64_t N, uint32_t n
 }
 
 // ------------------------------------------------------------ cell lookup
-__global__ void k_cell_start_tail(uint32_t* cell_start, uint32_t M, uint32_t N) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) cell_start[M] = N;
-}
-
 // Points per linear cell id (zero elsewhere); its exclusive scan is the
 // slot-prefix table ds: cell L holds slots [ds[L], ds[L+1]).
-__global__ void k_dense_counts(const uint64_t* __restrict__ cell_key, const uint32_t* __restrict__ sizes, uint32_t M,
-                               uint32_t* __restrict__ dcnt) {
+__global__ void k_dense_counts(const uint64_t* __restrict__ cell_key, const uint32_t* __restrict__ cell_start,
+                               uint32_t M, uint32_t* __restrict__ dcnt) {
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < M) dcnt[cell_key[c]] = sizes[c];
+    if (c < M) dcnt[cell_key[c]] = cell_start[c + 1] - cell_start[c];
 }
 
 __global__ void k_hash_insert(const uint64_t* __restrict__ cell_key, uint32_t M, unsigned long long* hkeys,
@@ -234,7 +230,7 @@ __global__ void k_item_counts(const uint32_t* __restrict__ cell_start, const uin
     const uint32_t c = order ? order[i] : i;
     const uint32_t sz = cell_start[c + 1] - cell_start[c];
     nchunks[i] = (sz + qchunk - 1) / qchunk;
-    if (sizes) sizes[i] = sz;
+    if (sizes) sizes[i] = ~sz;  // complemented: an ascending sort gives the descending order
 }
 
 __global__ void k_make_items(const uint32_t* __restrict__ order, const uint32_t* __restrict__ nchunks,
@@ -251,13 +247,7 @@ __global__ void k_iota(uint32_t* __restrict__ out, uint32_t M) {
     if (i < M) out[i] = i;
 }
 
-// Neighbour counts -> list lengths -> cursors.
-// List lengths in point-id order from the per-slot counts: total[ids[s]] = fwd[s] + rev[s].
-__global__ void k_sum_counts(const uint32_t* __restrict__ fwd, const uint32_t* __restrict__ rev,
-                             const uint32_t* __restrict__ ids, uint64_t N, uint32_t* __restrict__ total) {
-    const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (s < N) total[ids[s]] = fwd[s] + rev[s];
-}
+
 
 // ------------------------------------------------------------ launchers
 static inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
@@ -280,10 +270,10 @@ cudaError_t launch_minmax(const T* in, uint64_t N, uint32_t n, uint32_t k, const
     return cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, typename K>
 cudaError_t launch_cell_keys(const T* in, uint64_t N, uint32_t n, const uint32_t* perm, const GridGeom& g,
-                             const T* minArr, T eps, uint64_t* keys, uint32_t* vals, cudaStream_t st) {
-    k_cell_keys<T><<<blocks_for(N, 256), 256, 0, st>>>(in, N, n, perm, g, minArr, eps, keys, vals);
+                             const T* minArr, T eps, K* keys, uint32_t* vals, cudaStream_t st) {
+    k_cell_keys<T, K><<<blocks_for(N, 256), 256, 0, st>>>(in, N, n, perm, g, minArr, eps, keys, vals);
     return cudaGetLastError();
 }
 
@@ -294,11 +284,9 @@ cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t n
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, const uint32_t* sizes, uint32_t M,
-                               uint32_t N, uint32_t* dcnt, unsigned long long* hkeys, uint32_t* hvals,
-                               uint64_t hmask, cudaStream_t st) {
-    k_cell_start_tail<<<1, 32, 0, st>>>(cell_start, M, N);
-    if (dcnt) k_dense_counts<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, sizes, M, dcnt);
+cudaError_t launch_cell_tables(const uint64_t* cell_key, const uint32_t* cell_start, uint32_t M, uint32_t* dcnt,
+                               unsigned long long* hkeys, uint32_t* hvals, uint64_t hmask, cudaStream_t st) {
+    if (dcnt) k_dense_counts<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, cell_start, M, dcnt);
     if (hkeys) k_hash_insert<<<blocks_for(M, 256), 256, 0, st>>>(cell_key, M, hkeys, hvals, hmask);
     return cudaGetLastError();
 }
@@ -326,18 +314,17 @@ cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, const uint32_t* ids, uint64_t N,
-                              uint32_t* total, cudaStream_t st) {
-    k_sum_counts<<<blocks_for(N, 256), 256, 0, st>>>(fwd, rev, ids, N, total);
-    return cudaGetLastError();
-}
 
 #define GSJ_INST_INDEX(T)                                                                                  \
     template cudaError_t launch_variance<T>(const T*, uint64_t, uint32_t, T, T*, cudaStream_t);           \
     template cudaError_t launch_minmax<T>(const T*, uint64_t, uint32_t, uint32_t, const uint32_t*, T*,     \
                                           uint32_t, T*, cudaStream_t);                                     \
-    template cudaError_t launch_cell_keys<T>(const T*, uint64_t, uint32_t, const uint32_t*, const GridGeom&, \
-                                             const T*, T, uint64_t*, uint32_t*, cudaStream_t);             \
+    template cudaError_t launch_cell_keys<T, uint64_t>(const T*, uint64_t, uint32_t, const uint32_t*,      \
+                                                       const GridGeom&, const T*, T, uint64_t*, uint32_t*, \
+                                                       cudaStream_t);                                      \
+    template cudaError_t launch_cell_keys<T, uint32_t>(const T*, uint64_t, uint32_t, const uint32_t*,      \
+                                                       const GridGeom&, const T*, T, uint32_t*, uint32_t*, \
+                                                       cudaStream_t);                                      \
     template cudaError_t launch_gather_points<T>(const T*, uint64_t, uint32_t, uint32_t, const uint32_t*,  \
                                                  const uint32_t*, T*, cudaStream_t);
 GSJ_INST_INDEX(float)

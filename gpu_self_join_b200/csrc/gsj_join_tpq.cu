@@ -1,15 +1,28 @@
-// Thread-per-query join for dense low-dimensional grids (k <= 3).
+// Join of dense low-dimensional grids (k <= 3, n <= 4): the ROWS path.
 //
 // Low-dimensional workloads have tiny cells (a 2-D mixture of 20M points
 // averages 3 points per non-empty cell), so any per-cell set-up done by a
-// whole warp costs more than the distance tests.  Here each thread owns one
-// query slot; the slots of a warp are consecutive in cell order, so the lanes
-// of one cell walk identical candidate ranges (broadcast loads) and lanes of
-// neighbouring cells walk overlapping ones.  The neighbour rows come from the
-// cell plan (k_cell_plan): 3^(k-1) contiguous slot ranges, the full
-// neighbourhood of kernel.cu:292-302.  Every thread therefore finds exactly
-// its own neighbour set and counts it (k_rows_tpq); the fill pass (k_fill_q32)
-// spreads each query's candidates over a warp instead.
+// whole warp costs more than the distance tests.  Each query's candidates are
+// the 3^(k-1) contiguous slot ranges of its cell plan (k_cell_plan), the full
+// neighbourhood of kernel.cu:292-302, taken in a fixed order: candidate f of
+// query s is the f-th slot of the concatenated ranges.
+//
+//   k_rows_count  one thread per query slot (the slots of a warp are
+//                 consecutive in cell order, so lanes of one cell walk the same
+//                 ranges: broadcast loads).  It evaluates every candidate in the
+//                 reference's arithmetic and records the decisions as a bit
+//                 mask (bit f of the query's words), the list length by slot and
+//                 by point id.
+//   k_rows_fill   a warp per 32 consecutive query slots.  Each lane replays its
+//                 query's bit mask - no second distance pass - and writes the
+//                 hit ids to the warp's shared-memory stage at the query's
+//                 position within the warp's 32 lists; the warp then stores the
+//                 32 lists to their places in the point-id-ordered table, each
+//                 list with consecutive lanes.  A warp whose lists exceed the
+//                 stage is done in several windows.
+// Both kernels claim their 32-slot chunks dynamically (one atomic per warp,
+// the next claim issued before the current chunk is processed), since chunk
+// costs vary with the local density by orders of magnitude.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -20,255 +33,190 @@
 
 namespace gsj {
 
-template <typename T, int NT, int POL>
-__global__ void __launch_bounds__(256) k_rows_tpq(const JoinArgs<T> a, const uint32_t* __restrict__ slot_cell,
-                                                  uint32_t nrows) {
+namespace {
+
+// Next 32-slot chunk of the warp (lane 0 claims; the caller broadcasts it).
+__device__ __forceinline__ uint32_t claim32(uint32_t* ctr, int lane) {
+    uint32_t v = 0;
+    if (lane == 0) v = atomicAdd(ctr, 32u);
+    return v;
+}
+
+}  // namespace
+
+template <typename T, int NT, int NR, int POL>
+__global__ void __launch_bounds__(256) k_rows_count(const JoinArgs<T> a, const uint32_t* __restrict__ slot_cell,
+                                                    const uint64_t* __restrict__ bitoff, uint32_t* __restrict__ bits,
+                                                    uint32_t* __restrict__ counts_by_id) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const uint32_t N = a.n_points;
     const uint32_t npad = a.npad;
     unsigned long long cand = 0;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x) {
-        const uint32_t cell = slot_cell[s];
-        T q[NT];
-#pragma unroll
-        for (int l = 0; l < NT; l++) q[l] = a.pts[(size_t)s * npad + l];
-        uint32_t cnt = 0;
-        for (uint32_t r = 0; r < nrows; r++) {
-            const uint2 e = a.plan[(size_t)cell * nrows + r];
-            cand += e.y;
-            for (uint32_t i = 0; i < e.y; i++) {
-                const uint32_t c = e.x + i;
-                T cr[NT];
-#pragma unroll
-                for (int l = 0; l < NT; l++) cr[l] = a.pts[(size_t)c * npad + l];
-                const T d2 = sqdist_seq_reg<T, NT, POL>(q, cr);
-                if (d2 <= a.thr) cnt++;
-            }
-        }
-        a.fwd_cnt[s] = cnt;
-        a.rev_cnt[s] = 0u;
-    }
-    // one atomic per warp for the candidate statistic
-    for (int o = 16; o > 0; o >>= 1) cand += __shfl_down_sync(0xffffffffu, cand, o);
-    if ((threadIdx.x & 31) == 0 && cand) atomicAdd(a.cand_cnt, cand);
-}
-
-__device__ __forceinline__ unsigned lanemask_lt_q() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-// Fill pass of dense low-dimensional grids: a warp per 32 consecutive query
-// slots.  Lane j loads query j's coordinates, list cursor and the NR row
-// ranges of its cell in one parallel round; then the warp takes the queries
-// one after another, spreads the query's candidates over the lanes (32 per
-// tile) and writes its hits with one ballot per tile at consecutive positions
-// of the query's list.  Consecutive queries usually share a cell; while they
-// do, up to G candidate tiles stay in registers.  No per-cell set-up, no
-// shared memory, every list written by one warp in candidate order.
-template <typename T, int NT, int NR, int POL>
-__global__ void __launch_bounds__(256) k_fill_q32(const JoinArgs<T> a, const uint32_t* __restrict__ slot_cell) {
-    constexpr int G = 4;
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = lanemask_lt_q();
-    const uint32_t N = a.n_points;
-    const uint32_t npad = a.npad;
-    const uint64_t gwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    for (uint64_t s0 = gw * 32u; s0 < N; s0 += gwarps * 32u) {
-        const uint32_t s = (uint32_t)s0 + lane;
-        const uint32_t nq = min(32u, N - (uint32_t)s0);
-        // lane j: query j's cell, coordinates, list (pointer + length from the count pass)
-        uint32_t my_cell = 0xffffffffu, my_lo[NR], my_cnt[NR], my_len = 0;
-        T myq[NT];
-        uint32_t* my_list = a.table;
-        if ((uint32_t)lane < nq) {
-            my_cell = slot_cell[s];
-#pragma unroll
-            for (int l = 0; l < NT; l++) myq[l] = a.pts[(size_t)s * npad + l];
-            const unsigned long long off = a.offsets[a.ids[s]];
-            my_len = a.fwd_cnt[s] + a.rev_cnt[s];
-            if (off + my_len <= a.table_cap) my_list = a.table + off;
-            else {
-                my_len = 0;
-                *a.err_flag = 1u;
-            }
-#pragma unroll
-            for (int r = 0; r < NR; r++) {
-                const uint2 e = a.plan[(size_t)my_cell * NR + r];
-                my_lo[r] = e.x;
-                my_cnt[r] = e.y;
-            }
-        } else {
-#pragma unroll
-            for (int l = 0; l < NT; l++) myq[l] = T(0);
-#pragma unroll
-            for (int r = 0; r < NR; r++) my_lo[r] = my_cnt[r] = 0u;
-        }
-        uint32_t cached = 0xffffffffu, total = 0, ntile = 0;
-        uint32_t lo[NR], pre[NR + 1];
-        T cx[G][NT];
-        uint32_t cid[G];
-        bool cval[G];
-#pragma unroll
-        for (int r = 0; r < NR; r++) lo[r] = pre[r] = 0u;
-        pre[NR] = 0u;
-#pragma unroll
-        for (int t = 0; t < G; t++) {
-            cid[t] = 0u;
-            cval[t] = false;
-#pragma unroll
-            for (int l = 0; l < NT; l++) cx[t][l] = T(0);
-        }
-        for (uint32_t j = 0; j < nq; j++) {
-            const uint32_t cell = __shfl_sync(FULL, my_cell, j);
-            if (cell != cached) {
-                cached = cell;
-#pragma unroll
-                for (int r = 0; r < NR; r++) {
-                    lo[r] = __shfl_sync(FULL, my_lo[r], j);
-                    pre[r + 1] = pre[r] + __shfl_sync(FULL, my_cnt[r], j);
-                }
-                total = pre[NR];
-                ntile = (total + 31u) / 32u;
-                if (ntile <= (uint32_t)G) {
-#pragma unroll
-                    for (int t = 0; t < G; t++) {
-                        const uint32_t f = (uint32_t)t * 32u + lane;
-                        cval[t] = f < total;
-                        uint32_t slot = 0;
-                        if (cval[t]) {
-                            uint32_t st = lo[0], p = 0;
-#pragma unroll
-                            for (int rr = 1; rr < NR; rr++)
-                                if (f >= pre[rr]) {
-                                    st = lo[rr];
-                                    p = pre[rr];
-                                }
-                            slot = st + (f - p);
-                            cid[t] = a.ids[slot];
-                        }
-#pragma unroll
-                        for (int l = 0; l < NT; l++) cx[t][l] = a.pts[(size_t)slot * npad + l];
-                    }
-                }
-            }
+    uint32_t cur = __shfl_sync(FULL, claim32(a.work_counter, lane), 0);
+    while (cur < N) {
+        const uint32_t nxt = claim32(a.work_counter, lane);  // in flight while this chunk runs
+        const uint32_t s = cur + (uint32_t)lane;
+        if (s < N) {
+            const uint32_t cell = slot_cell[s];
             T q[NT];
 #pragma unroll
-            for (int l = 0; l < NT; l++) q[l] = __shfl_sync(FULL, myq[l], j);
-            uint32_t* list = reinterpret_cast<uint32_t*>(
-                __shfl_sync(FULL, reinterpret_cast<unsigned long long>(my_list), j));
-            const uint32_t len = __shfl_sync(FULL, my_len, j);
-            uint32_t run = 0;  // entries of this list written so far
-            if (ntile <= (uint32_t)G) {
+            for (int l = 0; l < NT; l++) q[l] = a.pts[(size_t)s * npad + l];
+            uint64_t wp = bitoff[s];
+            uint32_t cnt = 0, word = 0, f = 0;
 #pragma unroll
-                for (int t = 0; t < G; t++) {
-                    if ((uint32_t)t < ntile) {
-                        const T d2 = sqdist_seq_reg<T, NT, POL>(q, cx[t]);
-                        const bool hit = cval[t] && (d2 <= a.thr);
-                        const unsigned b = __ballot_sync(FULL, hit);
-                        const uint32_t pos = run + __popc(b & lt);
-                        if (hit && pos < len) list[pos] = cid[t];
-                        run += __popc(b);
+            for (int r = 0; r < NR; r++) {
+                const uint2 e = a.plan[(size_t)cell * NR + r];
+                for (uint32_t i = 0; i < e.y; i++) {
+                    const uint32_t c = e.x + i;
+                    T cr[NT];
+#pragma unroll
+                    for (int l = 0; l < NT; l++) cr[l] = a.pts[(size_t)c * npad + l];
+                    const T d2 = sqdist_seq_reg<T, NT, POL>(q, cr);
+                    const uint32_t hit = d2 <= a.thr ? 1u : 0u;
+                    word |= hit << (f & 31u);
+                    cnt += hit;
+                    f++;
+                    if ((f & 31u) == 0u) {
+                        bits[wp++] = word;
+                        word = 0u;
                     }
-                }
-            } else {
-                for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
-                    const uint32_t f = t0 + lane;
-                    const bool v = f < total;
-                    uint32_t slot = 0, c_id = 0;
-                    if (v) {
-                        uint32_t st = lo[0], p = 0;
-#pragma unroll
-                        for (int rr = 1; rr < NR; rr++)
-                            if (f >= pre[rr]) {
-                                st = lo[rr];
-                                p = pre[rr];
-                            }
-                        slot = st + (f - p);
-                        c_id = a.ids[slot];
-                    }
-                    T c[NT];
-#pragma unroll
-                    for (int l = 0; l < NT; l++) c[l] = a.pts[(size_t)slot * npad + l];
-                    const T d2 = sqdist_seq_reg<T, NT, POL>(q, c);
-                    const bool hit = v && (d2 <= a.thr);
-                    const unsigned b = __ballot_sync(FULL, hit);
-                    const uint32_t pos = run + __popc(b & lt);
-                    if (hit && pos < len) list[pos] = c_id;
-                    run += __popc(b);
                 }
             }
-            // the count pass and this pass must agree on every list
-            if (lane == 0 && run != len) *a.err_flag = 1u;
+            if (f & 31u) bits[wp] = word;
+            a.fwd_cnt[s] = cnt;
+            counts_by_id[a.ids[s]] = cnt;
+            cand += f;
         }
+        cur = __shfl_sync(FULL, nxt, 0);
     }
+    // one atomic per warp for the candidate statistic
+    for (int o = 16; o > 0; o >>= 1) cand += __shfl_down_sync(FULL, cand, o);
+    if (lane == 0 && cand) atomicAdd(a.cand_cnt, cand);
+}
+
+// Queries: the slots qslots[0 .. nq) (all slots 0 .. nq-1 when qslots is
+// null); the list of point id i goes to a.table[offsets[i] - base].
+template <int NR, int CAP>
+__global__ void __launch_bounds__(128) k_rows_fill(const JoinArgs<float> a, const uint32_t* __restrict__ slot_cell,
+                                                   const uint64_t* __restrict__ bitoff,
+                                                   const uint32_t* __restrict__ bits,
+                                                   const uint32_t* __restrict__ qslots, uint32_t nq, uint64_t base) {
+    __shared__ uint32_t stage_all[4][CAP];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    uint32_t* stage = stage_all[threadIdx.x >> 5];
+    uint32_t cur = __shfl_sync(FULL, claim32(a.work_counter, lane), 0);
+    while (cur < nq) {
+        const uint32_t nxt = claim32(a.work_counter, lane);
+        const uint32_t j = cur + (uint32_t)lane;
+        const bool valid = j < nq;
+        const uint32_t s = valid ? (qslots ? qslots[j] : j) : 0u;
+        uint32_t cnt = 0, nw = 0;
+        uint64_t bo = 0;
+        unsigned long long dst = 0;
+        uint32_t lo[NR], pre[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) lo[r] = pre[r] = 0u;
+        if (valid) {
+            cnt = a.fwd_cnt[s];
+            bo = bitoff[s];
+            nw = (uint32_t)(bitoff[s + 1] - bo);
+            dst = a.offsets[a.ids[s]] - base;
+            if (dst + cnt > a.table_cap) {
+                *a.err_flag = 1u;
+                cnt = 0u;
+            }
+            const uint32_t cell = slot_cell[s];
+            uint32_t p = 0;
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                const uint2 e = a.plan[(size_t)cell * NR + r];
+                lo[r] = e.x;
+                pre[r] = p;
+                p += e.y;
+            }
+        }
+        // position of this lane's list among the warp's 32 lists
+        uint32_t x = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        const uint32_t total = __shfl_sync(FULL, x, 31);
+        const uint32_t my_off = x - cnt;
+        for (uint32_t w0 = 0; w0 < total; w0 += (uint32_t)CAP) {
+            const uint32_t w1 = w0 + (uint32_t)CAP;
+            if (cnt && my_off < w1 && my_off + cnt > w0) {
+                uint32_t k = my_off;  // position of the next hit
+                for (uint32_t t = 0; t < nw && k < w1; t++) {
+                    uint32_t word = bits[bo + t];
+                    const uint32_t pc = (uint32_t)__popc(word);
+                    if (k + pc <= w0) {
+                        k += pc;
+                        continue;
+                    }
+                    while (word) {
+                        const uint32_t b = (uint32_t)(__ffs(word) - 1);
+                        word &= word - 1u;
+                        if (k >= w0 && k < w1) {
+                            const uint32_t f = t * 32u + b;
+                            uint32_t st = lo[0] + f;
+#pragma unroll
+                            for (int r = 1; r < NR; r++)
+                                if (f >= pre[r]) st = lo[r] + (f - pre[r]);
+                            stage[k - w0] = a.ids[st];
+                        }
+                        k++;
+                    }
+                }
+            }
+            __syncwarp();
+            // the warp stores the window's part of each list with consecutive lanes
+            for (int jj = 0; jj < 32; jj++) {
+                const uint32_t oj = __shfl_sync(FULL, my_off, jj);
+                const uint32_t cj = __shfl_sync(FULL, cnt, jj);
+                const unsigned long long dj = __shfl_sync(FULL, dst, jj);
+                const uint32_t b0 = oj > w0 ? oj : w0;
+                const uint32_t e0 = (oj + cj) < w1 ? (oj + cj) : w1;
+                for (uint32_t p = b0 + (uint32_t)lane; p < e0; p += 32u) a.table[dj + (p - oj)] = stage[p - w0];
+            }
+            __syncwarp();
+        }
+        cur = __shfl_sync(FULL, nxt, 0);
+    }
+}
+
+// Resident CTAs of a kernel, for persistent grids.
+static int resident_blocks(const void* kern, int threads, size_t smem, int num_sms) {
+    int per_sm = 0;
+    if (blocks_per_sm(kern, threads, smem, &per_sm) != cudaSuccess || per_sm < 1) per_sm = 1;
+    return num_sms * per_sm;
 }
 
 template <typename T, int NT, int NR>
-static cudaError_t launch_fill_q32_nt(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st) {
+static cudaError_t launch_count_nt(const JoinArgs<T>& a, const uint32_t* slot_cell, const uint64_t* bitoff,
+                                   uint32_t* bits, uint32_t* counts_by_id, int num_sms, cudaStream_t st) {
     constexpr int POL = sizeof(T) == 8 ? kPolF64 : kPolF32;
-    auto kern = k_fill_q32<T, NT, NR, POL>;
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    uint64_t blocks = (uint64_t)num_sms * per_sm * 4;
+    auto kern = k_rows_count<T, NT, NR, POL>;
+    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, 256, 0, num_sms);
     const uint64_t needed = ((uint64_t)a.n_points + 255) / 256;
     if (blocks > needed) blocks = needed ? needed : 1;
-    kern<<<(unsigned)blocks, 256, 0, st>>>(a, slot_cell);
+    kern<<<(unsigned)blocks, 256, 0, st>>>(a, slot_cell, bitoff, bits, counts_by_id);
     return cudaGetLastError();
 }
 
 template <typename T, int NR>
-static cudaError_t fill_q32_nr(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st) {
+static cudaError_t count_nr(const JoinArgs<T>& a, const uint32_t* slot_cell, const uint64_t* bitoff, uint32_t* bits,
+                            uint32_t* counts_by_id, int num_sms, cudaStream_t st) {
     switch (a.n) {
-        case 1: return launch_fill_q32_nt<T, 1, NR>(a, slot_cell, num_sms, st);
-        case 2: return launch_fill_q32_nt<T, 2, NR>(a, slot_cell, num_sms, st);
-        case 3: return launch_fill_q32_nt<T, 3, NR>(a, slot_cell, num_sms, st);
-        case 4: return launch_fill_q32_nt<T, 4, NR>(a, slot_cell, num_sms, st);
+        case 1: return launch_count_nt<T, 1, NR>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
+        case 2: return launch_count_nt<T, 2, NR>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
+        case 3: return launch_count_nt<T, 3, NR>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
+        case 4: return launch_count_nt<T, 4, NR>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
         default: return cudaErrorInvalidValue;
     }
-}
-
-template <typename T>
-cudaError_t launch_fill_q32(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st) {
-    if (!tpq_supported(a)) return cudaErrorInvalidValue;
-    if (a.g.k == 1) return fill_q32_nr<T, 1>(a, slot_cell, num_sms, st);
-    if (a.g.k == 2) return fill_q32_nr<T, 3>(a, slot_cell, num_sms, st);
-    return fill_q32_nr<T, 9>(a, slot_cell, num_sms, st);
-}
-
-template cudaError_t launch_fill_q32<float>(const JoinArgs<float>&, const uint32_t*, int, cudaStream_t);
-template cudaError_t launch_fill_q32<double>(const JoinArgs<double>&, const uint32_t*, int, cudaStream_t);
-
-// Slot -> cell index map (one thread per cell writes its slots).
-__global__ void k_slot_cell(const uint32_t* __restrict__ cell_start, uint32_t M, uint32_t* __restrict__ slot_cell) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= M) return;
-    for (uint32_t s = cell_start[c]; s < cell_start[c + 1]; s++) slot_cell[s] = c;
-}
-
-cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, uint32_t* slot_cell, cudaStream_t st) {
-    k_slot_cell<<<(M + 255) / 256, 256, 0, st>>>(cell_start, M, slot_cell);
-    return cudaGetLastError();
-}
-
-template <typename T, int NT>
-static cudaError_t launch_tpq_nt(const JoinArgs<T>& a, const uint32_t* slot_cell, uint32_t nrows, int num_sms,
-                                 cudaStream_t st) {
-    constexpr int POL = sizeof(T) == 8 ? kPolF64 : kPolF32;
-    auto kern = k_rows_tpq<T, NT, POL>;
-    int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    uint64_t blocks = (uint64_t)num_sms * per_sm;
-    const uint64_t needed = ((uint64_t)a.n_points + 255) / 256;
-    if (blocks > needed) blocks = needed ? needed : 1;
-    kern<<<(unsigned)blocks, 256, 0, st>>>(a, slot_cell, nrows);
-    return cudaGetLastError();
 }
 
 template <typename T>
@@ -277,21 +225,176 @@ bool tpq_supported(const JoinArgs<T>& a) {
 }
 
 template <typename T>
-cudaError_t launch_count_tpq(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st) {
+cudaError_t launch_rows_count(const JoinArgs<T>& a, const uint32_t* slot_cell, const uint64_t* bitoff, uint32_t* bits,
+                              uint32_t* counts_by_id, int num_sms, cudaStream_t st) {
     if (!tpq_supported(a)) return cudaErrorInvalidValue;
-    const uint32_t nrows = a.g.k == 1 ? 1u : (a.g.k == 2 ? 3u : 9u);
-    switch (a.n) {
-        case 1: return launch_tpq_nt<T, 1>(a, slot_cell, nrows, num_sms, st);
-        case 2: return launch_tpq_nt<T, 2>(a, slot_cell, nrows, num_sms, st);
-        case 3: return launch_tpq_nt<T, 3>(a, slot_cell, nrows, num_sms, st);
-        case 4: return launch_tpq_nt<T, 4>(a, slot_cell, nrows, num_sms, st);
-        default: return cudaErrorInvalidValue;
-    }
+    if (a.g.k == 1) return count_nr<T, 1>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
+    if (a.g.k == 2) return count_nr<T, 3>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
+    return count_nr<T, 9>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
+}
+
+constexpr int kFillCap = 2048;  // stage entries per warp (8 KB)
+
+template <int NR>
+static cudaError_t fill_nr(const JoinArgs<float>& a, const uint32_t* slot_cell, const uint64_t* bitoff,
+                           const uint32_t* bits, const uint32_t* qslots, uint32_t nq, uint64_t base, int num_sms,
+                           cudaStream_t st) {
+    if (nq == 0) return cudaSuccess;
+    auto kern = k_rows_fill<NR, kFillCap>;
+    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, 128, 0, num_sms);
+    const uint64_t needed = ((uint64_t)nq + 127) / 128;
+    if (blocks > needed) blocks = needed ? needed : 1;
+    kern<<<(unsigned)blocks, 128, 0, st>>>(a, slot_cell, bitoff, bits, qslots, nq, base);
+    return cudaGetLastError();
+}
+
+// The fill pass reads no coordinates: the table, offsets, ids and plan are
+// independent of the coordinate type, so both precisions share one kernel
+// (JoinArgs<float> view of the same buffers).
+template <typename T>
+cudaError_t launch_rows_fill(const JoinArgs<T>& a, const uint32_t* slot_cell, const uint64_t* bitoff,
+                             const uint32_t* bits, const uint32_t* qslots, uint32_t nq, uint64_t base, int num_sms,
+                             cudaStream_t st) {
+    if (!tpq_supported(a)) return cudaErrorInvalidValue;
+    JoinArgs<float> f{};
+    f.ids = a.ids;
+    f.plan = a.plan;
+    f.work_counter = a.work_counter;
+    f.n_points = a.n_points;
+    f.fwd_cnt = a.fwd_cnt;
+    f.offsets = a.offsets;
+    f.table = a.table;
+    f.table_cap = a.table_cap;
+    f.err_flag = a.err_flag;
+    if (a.g.k == 1) return fill_nr<1>(f, slot_cell, bitoff, bits, qslots, nq, base, num_sms, st);
+    if (a.g.k == 2) return fill_nr<3>(f, slot_cell, bitoff, bits, qslots, nq, base, num_sms, st);
+    return fill_nr<9>(f, slot_cell, bitoff, bits, qslots, nq, base, num_sms, st);
 }
 
 template bool tpq_supported<float>(const JoinArgs<float>&);
 template bool tpq_supported<double>(const JoinArgs<double>&);
-template cudaError_t launch_count_tpq<float>(const JoinArgs<float>&, const uint32_t*, int, cudaStream_t);
-template cudaError_t launch_count_tpq<double>(const JoinArgs<double>&, const uint32_t*, int, cudaStream_t);
+template cudaError_t launch_rows_count<float>(const JoinArgs<float>&, const uint32_t*, const uint64_t*, uint32_t*,
+                                              uint32_t*, int, cudaStream_t);
+template cudaError_t launch_rows_count<double>(const JoinArgs<double>&, const uint32_t*, const uint64_t*, uint32_t*,
+                                               uint32_t*, int, cudaStream_t);
+template cudaError_t launch_rows_fill<float>(const JoinArgs<float>&, const uint32_t*, const uint64_t*,
+                                             const uint32_t*, const uint32_t*, uint32_t, uint64_t, int, cudaStream_t);
+template cudaError_t launch_rows_fill<double>(const JoinArgs<double>&, const uint32_t*, const uint64_t*,
+                                              const uint32_t*, const uint32_t*, uint32_t, uint64_t, int,
+                                              cudaStream_t);
+
+// ---------------------------------------------------------------- result batches
+// Batch b of the host-result pipeline holds the point ids [bound[b],
+// bound[b+1]): its lists are the table range [boff[b], boff[b+1]) with boff[b]
+// = offsets[bound[b]].  bound[b] = the last id whose list starts at or below
+// b * step, so with step = segment capacity minus the longest list every batch
+// fits one segment; bound[0] = 0, bound[nb] = N.
+__global__ void k_batch_bounds(const uint64_t* __restrict__ offsets, uint32_t N, uint64_t step, uint32_t nb,
+                               uint32_t* __restrict__ bound, unsigned long long* __restrict__ boff) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nb) return;
+    if (b == 0 || b == nb) {
+        bound[b] = b == 0 ? 0u : N;
+        boff[b] = b == 0 ? 0ull : offsets[N];
+        return;
+    }
+    const unsigned long long target = (unsigned long long)b * step;
+    uint32_t lo = 0, hi = N;  // first i in [0, N) with offsets[i] > target (N if none)
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (offsets[mid] > target) hi = mid;
+        else lo = mid + 1u;
+    }
+    bound[b] = lo > 0 ? lo - 1u : 0u;
+    boff[b] = offsets[bound[b]];
+}
+
+// Batch index of every slot's point id (binary search over the bounds), and
+// the slot index as the value of the stable sort by batch.
+__global__ void k_slot_batch(const uint32_t* __restrict__ ids, uint32_t N, const uint32_t* __restrict__ bound,
+                             uint32_t nb, uint32_t* __restrict__ bkey, uint32_t* __restrict__ slot) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    const uint32_t id = ids[s];
+    uint32_t lo = 0, hi = nb;  // last b with bound[b] <= id
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) / 2u;
+        if (bound[mid] <= id) lo = mid;
+        else hi = mid;
+    }
+    bkey[s] = lo;
+    slot[s] = s;
+}
+
+// Start of each batch's slots in the batch-sorted slot list: gstart[b] =
+// first position whose batch key is >= b, gstart[nb] = N.
+__global__ void k_group_starts(const uint32_t* __restrict__ sorted_bkey, uint32_t N, uint32_t nb,
+                               uint32_t* __restrict__ gstart) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nb) return;
+    uint32_t lo = 0, hi = N;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (sorted_bkey[mid] >= b) hi = mid;
+        else lo = mid + 1u;
+    }
+    gstart[b] = lo;
+}
+
+// *out = max(in[0 .. n)) (*out zeroed by the caller).
+__global__ void k_max_u32(const uint32_t* __restrict__ in, uint64_t n, uint32_t* __restrict__ out) {
+    uint32_t m = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        m = max(m, in[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+cudaError_t launch_batch_bounds(const uint64_t* offsets, uint32_t N, uint64_t step, uint32_t nb, uint32_t* bound,
+                                unsigned long long* boff, cudaStream_t st) {
+    k_batch_bounds<<<(nb + 1 + 127) / 128, 128, 0, st>>>(offsets, N, step, nb, bound, boff);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slot_batch(const uint32_t* ids, uint32_t N, const uint32_t* bound, uint32_t nb, uint32_t* bkey,
+                              uint32_t* slot, cudaStream_t st) {
+    k_slot_batch<<<(N + 255) / 256, 256, 0, st>>>(ids, N, bound, nb, bkey, slot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_group_starts(const uint32_t* sorted_bkey, uint32_t N, uint32_t nb, uint32_t* gstart,
+                                cudaStream_t st) {
+    k_group_starts<<<(nb + 1 + 127) / 128, 128, 0, st>>>(sorted_bkey, N, nb, gstart);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_max_u32(const uint32_t* in, uint64_t n, uint32_t* out, cudaStream_t st) {
+    uint64_t blocks = (n + 255) / 256;
+    if (blocks > 1184) blocks = 1184;
+    k_max_u32<<<(unsigned)(blocks ? blocks : 1), 256, 0, st>>>(in, n, out);
+    return cudaGetLastError();
+}
+
+// Slot -> cell map and the bit-mask words of each slot's query: every query
+// of cell c has the same candidates, ceil(sum of its plan rows / 32) words.
+__global__ void k_slot_cell(const uint32_t* __restrict__ cell_start, uint32_t M, const uint2* __restrict__ plan,
+                            uint32_t nrows, uint32_t* __restrict__ slot_cell, uint32_t* __restrict__ swords) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= M) return;
+    uint64_t tot = 0;
+    if (swords)
+        for (uint32_t r = 0; r < nrows; r++) tot += plan[(size_t)c * nrows + r].y;
+    const uint32_t w = (uint32_t)((tot + 31u) / 32u);
+    for (uint32_t s = cell_start[c]; s < cell_start[c + 1]; s++) {
+        slot_cell[s] = c;
+        if (swords) swords[s] = w;
+    }
+}
+
+cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, const uint2* plan, uint32_t nrows,
+                             uint32_t* slot_cell, uint32_t* swords, cudaStream_t st) {
+    k_slot_cell<<<(M + 255) / 256, 256, 0, st>>>(cell_start, M, plan, nrows, slot_cell, swords);
+    return cudaGetLastError();
+}
 
 }  // namespace gsj

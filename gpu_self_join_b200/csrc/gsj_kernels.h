@@ -44,17 +44,18 @@ cudaError_t launch_variance(const T* in, uint64_t N, uint32_t n, T denom, T* var
 template <typename T>
 cudaError_t launch_minmax(const T* in, uint64_t N, uint32_t n, uint32_t k, const uint32_t* perm, T* part,
                           uint32_t nparts, T* out, cudaStream_t st);
-template <typename T>
+// Cell key per point (K = uint32_t when the grid has fewer than 2^32 cells)
+// and the point ids 0..N-1.
+template <typename T, typename K>
 cudaError_t launch_cell_keys(const T* in, uint64_t N, uint32_t n, const uint32_t* perm, const GridGeom& g,
-                             const T* minArr, T eps, uint64_t* keys, uint32_t* vals, cudaStream_t st);
+                             const T* minArr, T eps, K* keys, uint32_t* vals, cudaStream_t st);
 template <typename T>
 cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t npad, const uint32_t* perm,
                                  const uint32_t* ids, T* pts, cudaStream_t st);
-// cell_start[M] = N; then either the dense per-linear-id point counts
-// (dcnt[key] = size, to be scanned into the slot-prefix table) or the hash table.
-cudaError_t launch_cell_tables(const uint64_t* cell_key, uint32_t* cell_start, const uint32_t* sizes, uint32_t M,
-                               uint32_t N, uint32_t* dcnt, unsigned long long* hkeys, uint32_t* hvals,
-                               uint64_t hmask, cudaStream_t st);
+// Either the dense per-linear-id point counts (dcnt[key] = size, to be
+// scanned into the slot-prefix table) or the hash table of the non-empty cells.
+cudaError_t launch_cell_tables(const uint64_t* cell_key, const uint32_t* cell_start, uint32_t M, uint32_t* dcnt,
+                               unsigned long long* hkeys, uint32_t* hvals, uint64_t hmask, cudaStream_t st);
 cudaError_t launch_cell_plan(const uint64_t* cell_key, uint32_t M, const GridGeom& g, const uint32_t* ds,
                              uint2* plan, uint8_t* par, cudaStream_t st);
 cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order, uint32_t M, uint32_t qchunk,
@@ -62,8 +63,6 @@ cudaError_t launch_item_counts(const uint32_t* cell_start, const uint32_t* order
 cudaError_t launch_make_items(const uint32_t* order, const uint32_t* nchunks, const uint32_t* item_off,
                               uint32_t M, uint2* items, cudaStream_t st);
 cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st);
-cudaError_t launch_sum_counts(const uint32_t* fwd, const uint32_t* rev, const uint32_t* ids, uint64_t N,
-                              uint32_t* total, cudaStream_t st);
 
 // The warp-per-item join: appends packed pair keys into `o` (its rechecks
 // counter receives the exact number of keys; with o.emit false only that
@@ -76,15 +75,38 @@ template <typename T>
 cudaError_t launch_join_emit(const JoinArgs<T>& a, const TileOut& o, uint32_t nvisit, int model, bool stamp, bool rows,
                              int num_sms, cudaStream_t st);
 
-// Thread-per-query passes of dense low-dimensional grids (full neighbourhood).
-cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, uint32_t* slot_cell, cudaStream_t st);
+// ROWS path: dense low-dimensional grids (k <= 3, n <= 4), full neighbourhood.
+// slot_cell[s] = cell of slot s; with swords non-null also the bit-mask words
+// of slot s's query (ceil(candidates / 32); plan rows nrows per cell).
+cudaError_t launch_slot_cell(const uint32_t* cell_start, uint32_t M, const uint2* plan, uint32_t nrows,
+                             uint32_t* slot_cell, uint32_t* swords, cudaStream_t st);
 template <typename T>
 bool tpq_supported(const JoinArgs<T>& a);
+// Count pass (a.work_counter zeroed): a.fwd_cnt[s] and counts_by_id[ids[s]]
+// receive the list lengths, bits[bitoff[s] ...] the query's hit mask.
 template <typename T>
-cudaError_t launch_count_tpq(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st);
-// Fill pass of dense low-dimensional grids: a warp per 32 consecutive query slots.
+cudaError_t launch_rows_count(const JoinArgs<T>& a, const uint32_t* slot_cell, const uint64_t* bitoff, uint32_t* bits,
+                              uint32_t* counts_by_id, int num_sms, cudaStream_t st);
+// Fill pass (a.work_counter zeroed, a.offsets/table/table_cap/err_flag set):
+// replays the hit masks of the queries at slots qslots[0 .. nq) (slots
+// 0 .. nq-1 when qslots is null) into the point-id-ordered table; the list of
+// point id i lands at a.table[offsets[i] - base].
 template <typename T>
-cudaError_t launch_fill_q32(const JoinArgs<T>& a, const uint32_t* slot_cell, int num_sms, cudaStream_t st);
+cudaError_t launch_rows_fill(const JoinArgs<T>& a, const uint32_t* slot_cell, const uint64_t* bitoff,
+                             const uint32_t* bits, const uint32_t* qslots, uint32_t nq, uint64_t base, int num_sms,
+                             cudaStream_t st);
+// Result batches by point-id range: bound[0..nb] (ids) and boff[0..nb] (their
+// table offsets), each batch's lists at most `step` + the longest list
+// entries; per-slot batch keys (with the slot index as value, for a stable
+// sort by batch); the start of each batch in the sorted slot list.
+cudaError_t launch_batch_bounds(const uint64_t* offsets, uint32_t N, uint64_t step, uint32_t nb, uint32_t* bound,
+                                unsigned long long* boff, cudaStream_t st);
+cudaError_t launch_slot_batch(const uint32_t* ids, uint32_t N, const uint32_t* bound, uint32_t nb, uint32_t* bkey,
+                              uint32_t* slot, cudaStream_t st);
+cudaError_t launch_group_starts(const uint32_t* sorted_bkey, uint32_t N, uint32_t nb, uint32_t* gstart,
+                                cudaStream_t st);
+// *out = max of in[0 .. n) (*out zeroed by the caller).
+cudaError_t launch_max_u32(const uint32_t* in, uint64_t n, uint32_t* out, cudaStream_t st);
 
 // Tile join of high-dimensional float data (5 <= n <= kTileMaxN, k <= 6):
 // a CTA per item of up to kTileQ query slots; hits become packed

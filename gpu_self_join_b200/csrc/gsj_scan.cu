@@ -79,9 +79,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(unsigned long l
     if (threadIdx.x == 0) tsum[ntiles] = carry;
 }
 
+// OutT is uint64_t (list offsets) or uint32_t (slot offsets, digit offsets:
+// the caller guarantees that the total fits).
+template <typename OutT>
 __global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint32_t* __restrict__ in, uint64_t n,
                                                             const unsigned long long* __restrict__ tsum,
-                                                            uint64_t ntiles, uint64_t* __restrict__ out) {
+                                                            uint64_t ntiles, OutT* __restrict__ out) {
     // each thread owns kScanItems consecutive elements of the tile
     const uint64_t base = blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
@@ -97,25 +100,31 @@ __global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint32_t* __re
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
         const uint64_t e = base + i;
-        if (e < n) out[e] = run;
+        if (e < n) out[e] = (OutT)run;
         run += v[i];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tsum[ntiles];
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = (OutT)tsum[ntiles];
 }
 
 size_t scan_u32_u64_temp_bytes(uint64_t n) { return ((n + kScanTile - 1) / kScanTile + 1) * sizeof(unsigned long long); }
 
-cudaError_t scan_u32_u64(const uint32_t* in, uint64_t* out, uint64_t n, void* temp, cudaStream_t st) {
+template <typename OutT>
+static cudaError_t scan_any(const uint32_t* in, OutT* out, uint64_t n, void* temp, cudaStream_t st) {
     const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
     unsigned long long* tsum = static_cast<unsigned long long*>(temp);
-    if (ntiles == 0) {
-        cudaError_t e = cudaMemsetAsync(out, 0, sizeof(uint64_t), st);
-        return e;
-    }
+    if (ntiles == 0) return cudaMemsetAsync(out, 0, sizeof(OutT), st);
     k_tile_sums<<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, tsum);
     k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(tsum, ntiles);
-    k_tile_scan<<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, tsum, ntiles, out);
+    k_tile_scan<OutT><<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, tsum, ntiles, out);
     return cudaGetLastError();
+}
+
+cudaError_t scan_u32_u64(const uint32_t* in, uint64_t* out, uint64_t n, void* temp, cudaStream_t st) {
+    return scan_any<uint64_t>(in, out, n, temp, st);
+}
+
+cudaError_t scan_u32_u32(const uint32_t* in, uint32_t* out, uint64_t n, void* temp, cudaStream_t st) {
+    return scan_any<uint32_t>(in, out, n, temp, st);
 }
 
 // ---------------------------------------------------------------- no allocation
