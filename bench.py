@@ -143,44 +143,143 @@ def _traffic_from_profile(kernel: str, workload: str):
 def _roofline(stats: list, N: int, n: int, R: int, w) -> dict:
     """Roofline object for the join's dominant stage.  The device clock
     brackets two stages per join: "count" (ROWS: the count pass; the other
-    paths: sampling + the pair-emitting join) and "fill" (ROWS: the fill pass;
-    the other paths: pair sort + table).  Algorithmic bytes per launch:
-      join_fill   coordinates 4Nn + ids 4N + offsets 8N + table 4R
-      join_count  coordinates 4Nn + ids 4N + counts 4N (+ reverse counts 4N with STAMP)
+    paths: the estimate + the pair-emitting pass) and "fill" (ROWS: the fill
+    pass; the other paths: pair placement + list sort).  Algorithmic bytes per
+    launch (C = candidate evaluations):
+      join_fill   table 4R written, per-query list length, bit-mask offsets,
+                  id and list offset 24N, hit masks C/8 read
+      join_count  coordinates 4Nn, ids 4N, list lengths 8N (by slot and by id),
+                  hit masks C/8 written
       join_emit   coordinates 4Nn + ids 4N + 8-byte pair keys 8R
-      pair_sort   keys 8R read + table 4R + offsets 8N written
+      pair_place  keys 8R read + table 4R + offsets 8N written
     The screen is a tensor-core kernel: 2(n+2) FLOPs per screened pair (one
-    dot product of the n centred coordinates and the two norm columns)."""
+    dot product of the n centred coordinates and the two norm columns).
+    `join` is the whole join against the algorithmic bytes of the path,
+    4Nn + 4N + 4R (coordinates read once, numNeighbors and the table written)."""
     fill_ms = statistics.mean(s["dev_ms_fill"] for s in stats)
     count_ms = statistics.mean(s["dev_ms_count"] for s in stats)
+    index_ms = statistics.mean(s["dev_ms_index"] for s in stats)
+    C = float(stats[-1]["candidates"])
     path = int(stats[-1].get("join_path", 1))
     peak, peak_kind = _peaks()
     b_coords = 4.0 * N * n
     bound, unit, pk = "hbm", "GB/s", peak
     if path == 1:  # GSJ_PATH_ROWS
-        work_fill = b_coords + 4.0 * N + 8.0 * N + 4.0 * R
-        work_count = b_coords + 4.0 * N + 4.0 * N + (4.0 * N if w.stamp else 0.0)
+        work_fill = 4.0 * R + 24.0 * N + C / 8.0
+        work_count = b_coords + 4.0 * N + 8.0 * N + C / 8.0
         names = ("join_fill", "join_count")
     else:
         work_fill = 8.0 * R + 4.0 * R + 8.0 * N
         work_count = b_coords + 4.0 * N + 8.0 * R
-        names = ("pair_sort", "join_emit")
+        names = ("pair_place", "join_emit")
     if fill_ms >= count_ms:
         kname, kms, kwork = names[0], fill_ms, work_fill
     else:
         kname, kms, kwork = names[1], count_ms, work_count
         if path == 3:  # GSJ_PATH_SCREEN
             kname, bound, unit = "tile_screen", "tensor", "TFLOP/s"
-            kwork = 2.0 * (n + 2) * float(stats[-1]["candidates"])
+            kwork = 2.0 * (n + 2) * C
             pk, peak_kind = _tensor_peak()
     achieved = kwork / (kms / 1e3) / (1e12 if unit == "TFLOP/s" else 1e9)
+    join_ms = index_ms + count_ms + fill_ms
+    b_alg = b_coords + 4.0 * N + 4.0 * R
     roof = {"bound": bound, "kernel": kname, "achieved": achieved, "peak": pk, "unit": unit,
             "frac": achieved / pk, "peak_source": peak_kind,
             ("algorithmic_flops" if unit == "TFLOP/s" else "algorithmic_bytes"): kwork,
             "kernel_ms": kms, "traffic": _traffic_from_profile(kname, w.name),
-            "stage_ms": {"index": statistics.mean(s["dev_ms_index"] for s in stats), "count": count_ms,
-                         "fill": fill_ms}}
+            "stage_ms": {"index": index_ms, "count": count_ms, "fill": fill_ms},
+            "join": {"ms": join_ms, "algorithmic_bytes": b_alg, "achieved_gbs": b_alg / (join_ms / 1e3) / 1e9,
+                     "frac": b_alg / (join_ms / 1e3) / 1e9 / peak}}
     return roof
+
+
+def _link_peaks(nbytes: int) -> dict | None:
+    """Pinned host<->device copy bandwidth of this box (the host-link
+    roofline of the e2e number): best of 5 copies of nbytes each way."""
+    import torch
+
+    try:
+        dev = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+        res = {}
+        for name, fn in (("h2d_gbs", lambda: dev.copy_(host, non_blocking=True)),
+                         ("d2h_gbs", lambda: host.copy_(dev, non_blocking=True))):
+            best = None
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                fn()
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1)
+                best = t if best is None else min(best, t)
+            res[name] = nbytes / (best / 1e3) / 1e9
+        res["how"] = f"pinned copy of {nbytes} bytes each way, best of 5 (CUDA events)"
+        del dev, host
+        return res
+    except Exception:
+        return None
+
+
+def _screened_vs_plain(args, local_rank: int) -> dict:
+    """The metric's comparison: the tensor-core-screened join against the
+    plain exact FP32 join on the 18-D and 90-D workloads, end to end through
+    gsj_join_host (pinned host input and outputs), same step counts for both
+    arms, and both arms' outputs compared entry by entry."""
+    import torch
+
+    from gpu_self_join_b200 import JoinConfig, SelfJoin, synth
+
+    out = {}
+    for name in ("c4_derived18d", "c5_heavy90d"):
+        w = synth.WORKLOADS[name]
+        pts = synth.generate(name)
+        N, n = pts.shape
+        h_in = torch.from_numpy(pts).pin_memory().numpy()
+        res, tables = {}, {}
+        with SelfJoin(local_rank) as sj:
+            for arm, plain in (("screened", False), ("plain", True)):
+                cfg = JoinConfig(indexed_dims=w.k, reorder=w.reorder, shortcircuit=w.shortcircuit, ilp=w.ilp,
+                                 stamp=w.stamp, query_reorder=w.query_reorder, plain=plain)
+                st, _, _ = sj.run_host(h_in, w.eps, cfg)  # warm-up, gives the result size
+                R = int(st["total_pairs"])
+                hc = torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+                ht = torch.empty(max(R, 1), dtype=torch.int32).pin_memory().numpy().view(np.uint32)[:R]
+                sampler = ClockSampler(local_rank)
+                sampler.start()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                stats = []
+                e0.record()
+                for _ in range(args.sv_steps):
+                    stats.append(sj.run_host(h_in, w.eps, cfg, counts=hc, table=ht)[0])
+                e1.record()
+                torch.cuda.synchronize()
+                clocks = sampler.stop()
+                ms = e0.elapsed_time(e1) / args.sv_steps
+                s = stats[-1]
+                res[arm] = {"e2e_ms": ms, "pairs_per_s": R / (ms / 1e3), "result_pairs": R,
+                            "join_path": int(s["join_path"]), "stage_ms": {"index": s["dev_ms_index"],
+                            "count": s["dev_ms_count"], "fill": s["dev_ms_fill"]},
+                            "screen_rechecks": int(s["screen_rechecks"]), "candidates": int(s["candidates"]),
+                            "clocks": clocks}
+                if plain:
+                    # FP32 work of the reference's traversal: 3n FLOPs per candidate
+                    flops = 3.0 * n * s["candidates"]
+                    res[arm]["fp32_tflops"] = flops / (s["dev_ms_count"] / 1e3) / 1e12
+                else:
+                    tpk, kind = _tensor_peak()
+                    tf = 2.0 * (n + 2) * s["candidates"] / (s["dev_ms_count"] / 1e3) / 1e12
+                    res[arm]["tensor"] = {"tflops": tf, "peak": tpk, "frac": tf / tpk, "peak_source": kind}
+                tables[arm] = (hc.copy(), ht.copy())
+        same = (np.array_equal(tables["screened"][0], tables["plain"][0])
+                and np.array_equal(tables["screened"][1], tables["plain"][1]))
+        res["same_pairs"] = bool(same)
+        res["speedup_e2e"] = res["plain"]["e2e_ms"] / res["screened"]["e2e_ms"]
+        res["points"], res["dim"], res["eps"], res["steps"] = N, n, w.eps, args.sv_steps
+        out[name] = res
+        del tables
+    return out
 
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "rtree_harness")
@@ -379,30 +478,37 @@ def _ours(args) -> None:
     # ---- roofline of the dominant kernel
     roof = _roofline(stats, N, n, R, w)
 
-    # ---- e2e: host buffers through the public API
+    # ---- e2e: host buffers through the public API (gsj_join_host: pinned
+    # input, the table produced in batches that are copied to pinned host
+    # memory while the next batch is computed)
     e2e = None
     if not args.no_e2e:
         h_in = torch.from_numpy(pts).pin_memory().numpy()
         h_counts = torch.empty(N, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
         h_table = torch.empty(max(R, 1), dtype=torch.int32).pin_memory().numpy().view(np.uint32)[:R]
         for _ in range(max(1, min(args.warmup, 2))):
-            sj.run(h_in, w.eps, cfg)
-            sj.counts(out=h_counts)
-            sj.table(out=h_table)
+            sj.run_host(h_in, w.eps, cfg, counts=h_counts, table=h_table)
         barrier()
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record()
+        est = []
         for _ in range(args.steps):
-            sj.run(h_in, w.eps, cfg)
-            sj.counts(out=h_counts)
-            sj.table(out=h_table)
+            est.append(sj.run_host(h_in, w.eps, cfg, counts=h_counts, table=h_table)[0])
         f1.record()
         torch.cuda.synchronize()
         barrier()
         ems, _ = reduce_step(f0.elapsed_time(f1), 0.0, device="cuda")
+        d2h = int(4 * N + 4 * R)
         e2e = {"value": pairs_all / (ems / 1e3), "unit": "pairs/s", "ms_per_step": ems / args.steps,
-               "h2d_bytes_per_step": int(N * n * 4), "d2h_bytes_per_step": int(4 * N + 4 * R)}
+               "h2d_bytes_per_step": int(N * n * 4), "d2h_bytes_per_step": d2h,
+               "batches": int(est[-1]["batches"]), "api": "gsj_join_host (pinned host buffers)"}
+        link = _link_peaks(max(d2h, 1 << 26))
+        if link:
+            t_link = (N * n * 4) / (link["h2d_gbs"] * 1e9) + d2h / (link["d2h_gbs"] * 1e9)
+            e2e["roofline"] = {"bound": "host link", "h2d_gbs": link["h2d_gbs"], "d2h_gbs": link["d2h_gbs"],
+                               "link_ms": t_link * 1e3, "frac": t_link * 1e3 / (ems / args.steps),
+                               "how": link["how"]}
 
     launches = int(sum(s.get("kernel_launches", 0) for s in stats))
     line = {
@@ -420,6 +526,12 @@ def _ours(args) -> None:
                    "l2": "inputs (160 MB) and working set larger than L2"},
         "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
     }
+    if rank == 0 and world == 1 and args.workload == "c2_gmm2d" and not args.no_screened_vs_plain:
+        sj.close()
+        try:
+            line["screened_vs_plain"] = _screened_vs_plain(args, local_rank)
+        except Exception as ex:  # reported, never required for the headline line
+            line["screened_vs_plain"] = {"error": str(ex)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = _cpu_baseline(pts, w)
@@ -483,6 +595,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=256, help="joins in the c5_requests stream")
+    ap.add_argument("--no-screened-vs-plain", action="store_true",
+                    help="skip the 18-D / 90-D screened-versus-plain block of the default line")
+    ap.add_argument("--sv-steps", type=int, default=3, help="timed joins per arm of the screened-vs-plain block")
     ap.add_argument("--plain", action="store_true",
                     help="no tensor-core screen on high-dimensional workloads (exact FP32 for every pair)")
     args = ap.parse_args()

@@ -21,6 +21,9 @@ GSJ_FLAG_QUIET = 0x2
 GSJ_FLAG_NO_UNICOMP = 0x4
 GSJ_FLAG_PLAIN = 0x8
 GSJ_FLAG_EXACT_SIZE = 0x10
+GSJ_EST_SAMPLED = 0
+GSJ_EST_LEARNED = 1
+GSJ_ERR_OVERFLOW = -5
 
 # Every symbol declared in include/gpuselfjoin.h.
 EXPORTED_SYMBOLS = (
@@ -28,7 +31,11 @@ EXPORTED_SYMBOLS = (
     "gsj_result_size", "gsj_result_counts", "gsj_result_table", "gsj_result_device", "gsj_last_error",
     "gsj_threshold_f32", "gsj_threshold_f64", "GDSJoinPy", "copyResultIntoPythonArray", "GDSJoinPy_f32",
     "GDSJoinPy_f64", "copyResultIntoPythonArray64", "gsj_list_offsets_noalloc", "gsj_bruteforce_count",
+    "gsj_join_host", "gsj_model_train", "gsj_model_reset", "gsj_model_weights", "gsj_model_features",
+    "gsj_model_predict", "gsj_model_loss_grad",
 )
+MODEL_WEIGHTS = 3201
+MODEL_FEATURES = 16
 
 
 class GsjConfig(ctypes.Structure):
@@ -43,6 +50,11 @@ class GsjConfig(ctypes.Structure):
         ("query_reorder", ctypes.c_uint32),
         ("device", ctypes.c_int32),
         ("flags", ctypes.c_uint32),
+        ("buffer_pairs", ctypes.c_uint64),
+        ("streams", ctypes.c_uint32),
+        ("min_batches", ctypes.c_uint32),
+        ("estimator", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -66,6 +78,9 @@ class GsjStats(ctypes.Structure):
         ("join_path", ctypes.c_uint64),
         ("screen_rechecks", ctypes.c_uint64),
         ("reruns", ctypes.c_uint64),
+        ("batches", ctypes.c_uint64),
+        ("estimate", ctypes.c_uint64),
+        ("dev_ms_estimate", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -94,6 +109,8 @@ def lib() -> ctypes.CDLL:
     L.gsj_create.argtypes = [ctypes.POINTER(P), i32]
     L.gsj_destroy.argtypes = [P]
     L.gsj_join.argtypes = [P, P, u64, ctypes.c_double, ctypes.POINTER(GsjConfig), i32, ctypes.POINTER(GsjStats)]
+    L.gsj_join_host.argtypes = [P, P, u64, ctypes.c_double, ctypes.POINTER(GsjConfig), i32, P, P, u64,
+                                ctypes.POINTER(u64), ctypes.POINTER(GsjStats)]
     L.gsj_result_size.argtypes = [P, ctypes.POINTER(u64)]
     L.gsj_result_counts.argtypes = [P, P, i32]
     L.gsj_result_table.argtypes = [P, P, u64, i32]
@@ -110,6 +127,12 @@ def lib() -> ctypes.CDLL:
     L.gsj_list_offsets_noalloc.argtypes = [P, u64, P, P]
     L.gsj_bruteforce_count.argtypes = [P, P, u64, ctypes.c_double, ctypes.POINTER(GsjConfig), i32, P,
                                        ctypes.POINTER(u64)]
+    L.gsj_model_train.argtypes = [P, u32, P]
+    L.gsj_model_reset.argtypes = [P]
+    L.gsj_model_weights.argtypes = [P, P, u32, i32]
+    L.gsj_model_features.argtypes = [P, P, P, u32, ctypes.POINTER(u32)]
+    L.gsj_model_predict.argtypes = [P, P, u32, P]
+    L.gsj_model_loss_grad.argtypes = [P, P, P, u32, P, P]
     L.copyResultIntoPythonArray.argtypes = [P, ctypes.c_uint]
     L.copyResultIntoPythonArray.restype = None
     L.GDSJoinPy.restype = None

@@ -33,6 +33,7 @@
 #include "../../include/gpuselfjoin.h"
 #include "gsj_common.cuh"
 #include "gsj_kernels.h"
+#include "gsj_model.h"
 #include "gsj_place.h"
 #include "gsj_scan.h"
 #include "gsj_sort.h"
@@ -152,7 +153,7 @@ struct gsj_context {
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    cudaEvent_t tev[6] = {};  // stage timing: index start/end, count start/end, fill start/end
+    cudaEvent_t tev[8] = {};  // stage timing: index, count, fill (start/end), estimate start/end
     // device pool
     Buf in, pts, ids, keys, keys2, vals, cell_key, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
@@ -160,6 +161,25 @@ struct gsj_context {
         minmax_part, pairs, srows, snorms, spartial, scentre, unc, table2, nbtab, bitoff, hitbits, ptemp;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
+    // host-result pipeline: copy streams, per-segment events, pinned staging
+    static constexpr int kMaxSeg = 8;
+    cudaStream_t cst[kMaxSeg] = {};
+    cudaEvent_t seg_filled[kMaxSeg] = {}, seg_copied[kMaxSeg] = {};
+    PinnedBuf hseg[kMaxSeg];
+    Buf segs, bounds, bkeys;
+    bool table_on_device = true;  // false after a batched host-result join
+    // learned result-count model and the last join's cell table (its features)
+    Buf mw, mm1, mm2, mx, my, mxt, myt, mtmp;
+    bool model_ready = false;    // weights initialised
+    bool model_trained = false;  // trained on at least one join
+    uint32_t model_t = 0;        // Adam steps taken
+    double model_unc_ratio = 0;  // undecided / result pairs of the screen's training join (0: none)
+    struct {
+        bool valid = false;
+        uint32_t M = 0, n = 0;
+        float log2_eps = 0;
+        JoinArgs<float> lookup{};
+    } last;
     // last result
     bool have_result = false;
     uint64_t N = 0, R = 0;
@@ -401,11 +421,32 @@ int pairs_to_csr(gsj_context* c, unsigned long long* pairs, uint64_t nkeys, uint
         S.dev_ms_count = ms;
         GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[4], c->tev[5]));
         S.dev_ms_fill = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[6], c->tev[7]));
+        S.dev_ms_estimate = ms;
     }
     S.candidates = ncand;
     S.total_pairs = R;
     c->R = R;
     c->have_result = true;
+    return GSJ_OK;
+}
+
+// ------------------------------------------------------------------ learned estimate
+// Pairs the exact pass of the last indexed join will produce, predicted by the
+// context's model from the per-cell features (requires model_trained).
+int learned_estimate(gsj_context* c, double* est) {
+    cudaStream_t st = c->st;
+    const uint32_t M = c->last.M;
+    float* X = nullptr;
+    GSJ_TRY(dev_get(c, c->mx, (size_t)M * kModelFeatures, &X));
+    double* d_est = nullptr;
+    GSJ_TRY(dev_get(c, c->mtmp, 4, &d_est));
+    GSJ_CUDA(c, cudaMemsetAsync(d_est, 0, sizeof(double), st));
+    c->stats.kernel_launches += 2;
+    GSJ_CUDA(c, model_features(c->last.lookup, M, c->last.log2_eps, c->last.n, X, st));
+    GSJ_CUDA(c, model_predict(X, M, static_cast<const float*>(c->mw.p), nullptr, c->last.lookup.cell_start,
+                              (float)c->last.lookup.n_points, d_est, st));
+    GSJ_TRY(d2h_small(c, est, d_est, 1));
     return GSJ_OK;
 }
 
@@ -416,7 +457,8 @@ int pairs_to_csr(gsj_context* c, unsigned long long* pairs, uint64_t nkeys, uint
 // the keys are sorted into the table.
 template <typename T>
 int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model, bool rows, bool exact_size,
-              uint32_t* counts, uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
+              bool learned, uint32_t* counts, uint64_t* offsets, unsigned long long* cursor, double t_join,
+              double t_start) {
     constexpr uint32_t kSampleStride = 64;
     gsj_stats& S = c->stats;
     cudaStream_t st = c->st;
@@ -438,15 +480,24 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
         return GSJ_OK;
     };
     GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
-    const uint32_t nsample = (ni + kSampleStride - 1) / kSampleStride;
-    GSJ_TRY(reset());
-    o.emit = false;
-    o.stride = kSampleStride;
-    S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_join_emit<T>(a, o, nsample, model, stamp, rows, c->num_sms, st));
-    unsigned long long sampled = 0;
-    GSJ_TRY(d2h_small(c, &sampled, o.rechecks, 1));
-    const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
+    GSJ_CUDA(c, cudaEventRecord(c->tev[6], st));
+    double est = 0.0;
+    if (learned) {
+        GSJ_TRY(learned_estimate(c, &est));
+    } else if (!exact_size) {
+        // sampled estimator: the exact pass over every kSampleStride-th item
+        const uint32_t nsample = (ni + kSampleStride - 1) / kSampleStride;
+        GSJ_TRY(reset());
+        o.emit = false;
+        o.stride = kSampleStride;
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_join_emit<T>(a, o, nsample, model, stamp, rows, c->num_sms, st));
+        unsigned long long sampled = 0;
+        GSJ_TRY(d2h_small(c, &sampled, o.rechecks, 1));
+        est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
+    }
+    GSJ_CUDA(c, cudaEventRecord(c->tev[7], st));
+    S.estimate = (uint64_t)est;
     const uint64_t estimate = exact_size ? 0u : (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
     uint64_t cap = estimate;
     unsigned long long* pairs = nullptr;
@@ -481,7 +532,8 @@ int emit_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, bool stamp, int model,
 // buffer; the full pass counts every pair even past the buffer, so a short
 // buffer is re-sized to the exact count and the pass repeated.
 int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int model, bool screen, bool exact_size,
-              uint32_t* counts, uint64_t* offsets, unsigned long long* cursor, double t_join, double t_start) {
+              bool learned, uint32_t* counts, uint64_t* offsets, unsigned long long* cursor, double t_join,
+              double t_start) {
     constexpr uint32_t kSampleStride = 64;
     gsj_stats& S = c->stats;
     cudaStream_t st = c->st;
@@ -525,21 +577,30 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
         sc.rows = rows;
         sc.norms = norms;
     }
-    // ---- sampling pass
-    const uint32_t nsample = (ni + kSampleStride - 1) / kSampleStride;
-    GSJ_TRY(reset());
-    o.emit = false;
-    o.stride = kSampleStride;
-    S.kernel_launches += 1;
-    GSJ_CUDA(c, launch(nsample));
-    unsigned long long sampled = 0;
-    GSJ_TRY(d2h_small(c, &sampled, screen ? o.rechecks : cursor, 1));
-    {
+    // ---- estimate of the exact pass's entries (pairs, or the screen's undecided pairs)
+    if (learned && screen && !(c->model_unc_ratio > 0.0)) learned = false;  // no screened training join yet
+    GSJ_CUDA(c, cudaEventRecord(c->tev[6], st));
+    double est = 0.0;
+    if (learned) {
+        GSJ_TRY(learned_estimate(c, &est));
+        if (screen) est *= c->model_unc_ratio;
+    } else if (!exact_size) {
+        // sampled estimator: the exact pass over every kSampleStride-th item
+        const uint32_t nsample = (ni + kSampleStride - 1) / kSampleStride;
+        GSJ_TRY(reset());
+        o.emit = false;
+        o.stride = kSampleStride;
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch(nsample));
+        unsigned long long sampled = 0;
+        GSJ_TRY(d2h_small(c, &sampled, screen ? o.rechecks : cursor, 1));
         uint32_t err = 0;
         GSJ_TRY(d2h_small(c, &err, a.err_flag, 1));
         if (err) return fail(c, GSJ_ERR_CUDA, "tile join: tensor-core wait timed out");
+        est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
     }
-    const double est = nsample ? (double)sampled * (double)ni / (double)nsample : 0.0;
+    GSJ_CUDA(c, cudaEventRecord(c->tev[7], st));
+    S.estimate = (uint64_t)est;
     const uint64_t estimate = exact_size ? 0u : (uint64_t)(est * 1.25) + N + (1u << 16) + slack;
     uint64_t cap = estimate;
     // ---- full pass (repeated with a larger buffer if the buffer was short):
@@ -595,14 +656,160 @@ int tile_join(gsj_context* c, JoinArgs<float>& a, uint64_t N, bool stamp, int mo
     return GSJ_OK;
 }
 
+// ------------------------------------------------------------------ host results
+// Destination of gsj_join_host.
+struct HostOut {
+    uint32_t* counts;  // numNeighbors[N], host
+    uint32_t* table;   // neighborTable, host, `cap` entries
+    uint64_t cap;
+};
+
+int ensure_copy_streams(gsj_context* c, int nseg) {
+    for (int i = 0; i < nseg; i++) {
+        if (!c->cst[i]) GSJ_CUDA(c, cudaStreamCreateWithFlags(&c->cst[i], cudaStreamNonBlocking));
+        if (!c->seg_filled[i]) GSJ_CUDA(c, cudaEventCreateWithFlags(&c->seg_filled[i], cudaEventDisableTiming));
+        if (!c->seg_copied[i]) GSJ_CUDA(c, cudaEventCreateWithFlags(&c->seg_copied[i], cudaEventDisableTiming));
+    }
+    return GSJ_OK;
+}
+
+// ROWS path, results to the host: the table is filled in batches of point-id
+// ranges whose lists fit one device segment; each batch's segment is copied to
+// the host on its own copy stream while the compute stream fills the next
+// segment.  offsets/counts are final (the count pass is exact), so every batch
+// has a known place in the host table.
+template <typename T>
+int rows_to_host(gsj_context* c, JoinArgs<T>& a, const gsj_config& cfg, uint64_t N, uint64_t R,
+                 const uint32_t* slot_cell, const uint64_t* bitoff, const uint32_t* hitbits, const uint32_t* counts,
+                 const uint64_t* offsets, const HostOut& ho) {
+    gsj_stats& S = c->stats;
+    cudaStream_t st = c->st;
+    uint32_t* ctr = a.work_counter;
+    // numNeighbors to the host (overlaps the batches when the destination is pinned)
+    const bool counts_pinned = host_is_pinned(ho.counts);
+    const bool table_pinned = host_is_pinned(ho.table);
+    GSJ_CUDA(c, cudaEventRecord(c->ev[0], st));
+    if (counts_pinned) {
+        GSJ_CUDA(c, cudaStreamWaitEvent(c->st2, c->ev[0], 0));
+        GSJ_CUDA(c, cudaMemcpyAsync(ho.counts, counts, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st2));
+    }
+    // batch plan: segments of seg_cap entries, each batch at most seg_cap
+    uint64_t seg_cap = cfg.buffer_pairs ? cfg.buffer_pairs : 100000000ull;
+    const uint32_t min_b = cfg.min_batches ? cfg.min_batches : 3u;
+    uint32_t lmax = 0;
+    {
+        uint32_t* d_lmax = reinterpret_cast<uint32_t*>(c->misc.p) + 4 * kMaxK + 28;
+        GSJ_CUDA(c, cudaMemsetAsync(d_lmax, 0, sizeof(uint32_t), st));
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_max_u32(counts, N, d_lmax, st));
+        GSJ_TRY(d2h_small(c, &lmax, d_lmax, 1));
+    }
+    if (seg_cap < 2ull * lmax) seg_cap = 2ull * lmax;  // the longest list must fit with room
+    uint64_t step = seg_cap - lmax;
+    const uint64_t even = (R + min_b - 1) / min_b;
+    if (even >= 1 && even < step) step = even;
+    const uint64_t nb64 = R ? (R + step - 1) / step : 1;
+    if (nb64 > 65535) return fail(c, GSJ_ERR_INVALID, "more than 65535 result batches: raise buffer_pairs");
+    const uint32_t nb = (uint32_t)nb64;
+    S.batches = nb;
+    // bound[nb+1] and gstart[nb+1] (32-bit), then boff[nb+1] (64-bit)
+    unsigned long long* bbuf = nullptr;
+    GSJ_TRY(dev_get(c, c->bounds, 2ull * (nb + 1), &bbuf));
+    uint32_t* bound = reinterpret_cast<uint32_t*>(bbuf);
+    uint32_t* gstart = bound + (nb + 1);
+    unsigned long long* boff = bbuf + (nb + 1);
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_batch_bounds(offsets, (uint32_t)N, step, nb, bound, boff, st));
+    // the query slots grouped by batch (a stable sort keeps slot order inside a batch)
+    uint32_t *bkey = nullptr, *bkey2 = nullptr, *qs = nullptr, *qs2 = nullptr;
+    GSJ_TRY(dev_get(c, c->bkeys, 4ull * N, &bkey));
+    bkey2 = bkey + N;
+    qs = bkey + 2 * N;
+    qs2 = bkey + 3 * N;
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_slot_batch(a.ids, (uint32_t)N, bound, nb, bkey, qs, st));
+    int kb = 1;
+    while (kb < 32 && ((nb - 1) >> kb)) kb++;
+    void* temp = nullptr;
+    GSJ_TRY(dev_get(c, c->temp, radix_sort_temp_bytes(N), (unsigned char**)&temp));
+    bool alt = false;
+    int nl = 0;
+    if (nb > 1) GSJ_CUDA(c, radix_sort<uint32_t>(bkey, bkey2, qs, qs2, N, 0, kb, temp, &alt, &nl, st));
+    S.kernel_launches += (uint64_t)nl;
+    const uint32_t* sorted_key = alt ? bkey2 : bkey;
+    const uint32_t* qslots = alt ? qs2 : qs;
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_group_starts(sorted_key, (uint32_t)N, nb, gstart, st));
+    std::vector<uint32_t> h_gs(nb + 1);
+    std::vector<unsigned long long> h_bo(nb + 1);
+    GSJ_CUDA(c, cudaMemcpyAsync(h_gs.data(), gstart, (nb + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    GSJ_CUDA(c, cudaMemcpyAsync(h_bo.data(), boff, (nb + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                st));
+    GSJ_CUDA(c, cudaStreamSynchronize(st));
+    if (h_bo[nb] != R) return fail(c, GSJ_ERR_STATE, "result batches do not cover the table (internal error)");
+    // segments in flight
+    const int nseg = (int)std::min<uint32_t>(nb, std::min<uint32_t>(cfg.streams ? cfg.streams : 3u,
+                                                                      (uint32_t)gsj_context::kMaxSeg));
+    GSJ_TRY(ensure_copy_streams(c, nseg));
+    uint32_t* segs = nullptr;
+    GSJ_TRY(dev_get(c, c->segs, (size_t)nseg * seg_cap, &segs));
+    if (!table_pinned)
+        for (int i = 0; i < nseg; i++) GSJ_TRY(pinned_get(c, c->hseg[i], seg_cap * sizeof(uint32_t)));
+    a.table_cap = seg_cap;
+    a.err_flag = ctr + 1;
+    GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
+    // pageable destinations: the staged batches are copied out in order
+    uint32_t next_out = 0;
+    auto drain = [&](uint32_t upto) -> int {
+        for (; next_out < upto; next_out++) {
+            const int sg = (int)(next_out % (uint32_t)nseg);
+            GSJ_CUDA(c, cudaEventSynchronize(c->seg_copied[sg]));
+            const uint64_t rb = h_bo[next_out + 1] - h_bo[next_out];
+            par_memcpy(ho.table + h_bo[next_out], c->hseg[sg].p, rb * sizeof(uint32_t));
+        }
+        return GSJ_OK;
+    };
+    for (uint32_t b = 0; b < nb; b++) {
+        const int sg = (int)(b % (uint32_t)nseg);
+        if (b >= (uint32_t)nseg) {
+            if (!table_pinned) GSJ_TRY(drain(b - (uint32_t)nseg + 1));  // frees the staging buffer
+            GSJ_CUDA(c, cudaStreamWaitEvent(st, c->seg_copied[sg], 0));
+        }
+        uint32_t* seg = segs + (size_t)sg * seg_cap;
+        a.table = seg;
+        GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st));
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_rows_fill<T>(a, slot_cell, bitoff, hitbits, qslots + h_gs[b], h_gs[b + 1] - h_gs[b],
+                                        h_bo[b], c->num_sms, st));
+        GSJ_CUDA(c, cudaEventRecord(c->seg_filled[sg], st));
+        const uint64_t rb = h_bo[b + 1] - h_bo[b];
+        GSJ_CUDA(c, cudaStreamWaitEvent(c->cst[sg], c->seg_filled[sg], 0));
+        if (rb)
+            GSJ_CUDA(c, cudaMemcpyAsync(table_pinned ? (void*)(ho.table + h_bo[b]) : c->hseg[sg].p, seg,
+                                        rb * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->cst[sg]));
+        GSJ_CUDA(c, cudaEventRecord(c->seg_copied[sg], c->cst[sg]));
+    }
+    GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
+    if (!table_pinned) GSJ_TRY(drain(nb));
+    for (int i = 0; i < nseg; i++) GSJ_CUDA(c, cudaStreamSynchronize(c->cst[i]));
+    GSJ_CUDA(c, cudaStreamSynchronize(st));
+    if (counts_pinned) GSJ_CUDA(c, cudaStreamSynchronize(c->st2));
+    else GSJ_TRY(d2h_staged(c, ho.counts, counts, N * sizeof(uint32_t)));
+    return GSJ_OK;
+}
+
 // ------------------------------------------------------------------ join
 template <typename T>
-int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const gsj_config& cfg, int on_dev) {
+int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const gsj_config& cfg, int on_dev,
+             const HostOut* ho) {
     const double t_start = now_ms();
     gsj_stats& S = c->stats;
     S = gsj_stats{};
     S.num_points = N;
     c->have_result = false;
+    c->table_on_device = true;
+    c->last.valid = false;
+    S.batches = 1;
     c->N = N;
     c->R = 0;
     const T eps = (T)eps_d;
@@ -930,16 +1137,35 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     a.cand_cnt = cand;
     const bool stamp = cfg.stamp != 0 && !(cfg.flags & GSJ_FLAG_NO_UNICOMP);
     const bool exact_size = (cfg.flags & GSJ_FLAG_EXACT_SIZE) != 0;
+    // the cell table of this join, for the model's features (estimate now,
+    // training after the join)
+    c->last.valid = true;
+    c->last.M = M;
+    c->last.n = n;
+    c->last.log2_eps = (float)std::log2((double)eps);
+    c->last.lookup = JoinArgs<float>{};
+    c->last.lookup.cell_start = cell_start;
+    c->last.lookup.cell_key = cell_key;
+    c->last.lookup.ds = ds;
+    c->last.lookup.hkeys = reinterpret_cast<const uint64_t*>(hkeys);
+    c->last.lookup.hvals = hvals;
+    c->last.lookup.hmask = hmask;
+    c->last.lookup.g = g;
+    c->last.lookup.n_points = (uint32_t)N;
+    c->last.lookup.ids = ids;
+    const bool learned = !exact_size && cfg.estimator == GSJ_EST_LEARNED && c->model_trained;
     if constexpr (std::is_same<T, float>::value) {
         if (tile) {
             unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
-            return tile_join(c, a, N, stamp, model, screen, exact_size, counts, offsets, cursor, t_join, t_start);
+            return tile_join(c, a, N, stamp, model, screen, exact_size, learned, counts, offsets, cursor, t_join,
+                             t_start);
         }
     }
     // Every other grid except the thread-per-query rows: one emit pass + pair sort.
     if (!tpq) {
         unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
-        return emit_join<T>(c, a, N, stamp, model, rows, exact_size, counts, offsets, cursor, t_join, t_start);
+        return emit_join<T>(c, a, N, stamp, model, rows, exact_size, learned, counts, offsets, cursor, t_join,
+                            t_start);
     }
     // Dense low-dimensional grids (the ROWS path): the distance work is cheap
     // and the cells too small for per-cell warp work, so one thread per query
@@ -967,7 +1193,36 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     GSJ_TRY(d2h_small(c, &ncand, cand, 1));
     S.candidates = ncand;
 
-    // ---- fill pass
+    // ---- fill pass: into the device table, or in batches to the host
+    if (ho) {
+        c->table_on_device = false;
+        if (ho->cap < R) {
+            GSJ_TRY(d2h_staged(c, ho->counts, counts, N * sizeof(uint32_t)));
+            S.total_pairs = R;
+            c->R = R;
+            return GSJ_ERR_OVERFLOW;
+        }
+        GSJ_TRY(rows_to_host<T>(c, a, cfg, N, R, slot_cell, bitoff, hitbits, counts, offsets, *ho));
+        {
+            float ms = 0;
+            GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
+            S.dev_ms_index = ms;
+            GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[2], c->tev[3]));
+            S.dev_ms_count = ms;
+            GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[4], c->tev[5]));
+            S.dev_ms_fill = ms;
+        }
+        uint32_t errflag = 0;
+        GSJ_TRY(d2h_small(c, &errflag, ctr + 1, 1));
+        if (errflag) return fail(c, GSJ_ERR_STATE, "fill pass: a list would leave its segment (internal error)");
+        S.ms_join = now_ms() - t_join;
+        S.total_pairs = R;
+        S.join_path = GSJ_PATH_ROWS;
+        c->R = R;
+        c->have_result = true;
+        S.ms_total = now_ms() - t_start;
+        return GSJ_OK;
+    }
     uint32_t* table = nullptr;
     GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
     GSJ_CUDA(c, cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st));
@@ -1094,6 +1349,16 @@ int gsj_destroy(gsj_context* c) {
         if (b->p) cudaFree(b->p);
     for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})
         if (pb->p) cudaFreeHost(pb->p);
+    for (int i = 0; i < gsj_context::kMaxSeg; i++) {
+        if (c->cst[i]) cudaStreamSynchronize(c->cst[i]);
+        if (c->hseg[i].p) cudaFreeHost(c->hseg[i].p);
+        if (c->seg_filled[i]) cudaEventDestroy(c->seg_filled[i]);
+        if (c->seg_copied[i]) cudaEventDestroy(c->seg_copied[i]);
+        if (c->cst[i]) cudaStreamDestroy(c->cst[i]);
+    }
+    for (Buf* b : {&c->segs, &c->bounds, &c->bkeys, &c->mw, &c->mm1, &c->mm2, &c->mx, &c->my, &c->mxt, &c->myt,
+                   &c->mtmp})
+        if (b->p) cudaFree(b->p);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->tev)
@@ -1111,8 +1376,42 @@ int gsj_join(gsj_context* c, const void* data, uint64_t num_points, double eps, 
     GSJ_TRY(validate(c, *cfg, num_points));
     if (cfg->device != c->device) return fail(c, GSJ_ERR_INVALID, "config device differs from the context's device");
     GSJ_CUDA(c, cudaSetDevice(c->device));
-    int r = cfg->dtype == GSJ_FLOAT32 ? run_join<float>(c, data, num_points, eps, *cfg, data_on_device)
-                                      : run_join<double>(c, data, num_points, eps, *cfg, data_on_device);
+    int r = cfg->dtype == GSJ_FLOAT32 ? run_join<float>(c, data, num_points, eps, *cfg, data_on_device, nullptr)
+                                      : run_join<double>(c, data, num_points, eps, *cfg, data_on_device, nullptr);
+    if (stats) *stats = c->stats;
+    return r;
+}
+
+int gsj_join_host(gsj_context* c, const void* data, uint64_t num_points, double eps, const gsj_config* cfg,
+                  int data_on_device, uint32_t* num_neighbors, uint32_t* neighbor_table, uint64_t cap,
+                  uint64_t* total_pairs, gsj_stats* stats) {
+    if (!c || !cfg || !total_pairs) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (!data && num_points) return fail(c, GSJ_ERR_INVALID, "null data");
+    if (!num_neighbors && num_points) return fail(c, GSJ_ERR_INVALID, "null num_neighbors");
+    if (!neighbor_table && cap) return fail(c, GSJ_ERR_INVALID, "null neighbor_table");
+    GSJ_TRY(validate(c, *cfg, num_points));
+    if (cfg->device != c->device) return fail(c, GSJ_ERR_INVALID, "config device differs from the context's device");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    *total_pairs = 0;
+    HostOut ho{num_neighbors, neighbor_table, cap};
+    const double t0 = now_ms();
+    int r = cfg->dtype == GSJ_FLOAT32 ? run_join<float>(c, data, num_points, eps, *cfg, data_on_device, &ho)
+                                      : run_join<double>(c, data, num_points, eps, *cfg, data_on_device, &ho);
+    if (r == GSJ_OK || r == GSJ_ERR_OVERFLOW) *total_pairs = c->R;
+    if (r == GSJ_OK && c->table_on_device && c->N) {
+        // paths without batches: the finished result is copied out
+        if (cap < c->R) {
+            r = d2h_staged(c, num_neighbors, c->counts.p, c->N * sizeof(uint32_t));
+            if (r == GSJ_OK) r = GSJ_ERR_OVERFLOW;
+        } else {
+            const double t1 = now_ms();
+            r = d2h_staged(c, num_neighbors, c->counts.p, c->N * sizeof(uint32_t));
+            if (r == GSJ_OK && c->R) r = d2h_staged(c, neighbor_table, c->table.p, c->R * sizeof(uint32_t));
+            c->stats.ms_d2h += now_ms() - t1;
+        }
+    }
+    if (r == GSJ_ERR_OVERFLOW) fail(c, r, "neighbor_table holds fewer entries than the result (see total_pairs)");
+    c->stats.ms_total = now_ms() - t0;
     if (stats) *stats = c->stats;
     return r;
 }
@@ -1187,6 +1486,7 @@ int gsj_result_counts(gsj_context* c, uint32_t* out, int dst_on_device) {
 int gsj_result_table(gsj_context* c, uint32_t* out, uint64_t cap, int dst_on_device) {
     if (!c || (!out && c->R)) return fail(c, GSJ_ERR_INVALID, "null argument");
     if (!c->have_result) return fail(c, GSJ_ERR_STATE, "no join result");
+    if (!c->table_on_device) return fail(c, GSJ_ERR_STATE, "the last join delivered its table to host memory");
     if (cap < c->R) return fail(c, GSJ_ERR_INVALID, "destination smaller than the result");
     GSJ_CUDA(c, cudaSetDevice(c->device));
     if (c->R == 0) return GSJ_OK;
@@ -1204,6 +1504,7 @@ int gsj_result_table(gsj_context* c, uint32_t* out, uint64_t cap, int dst_on_dev
 int gsj_result_device(gsj_context* c, const uint32_t** counts, const uint64_t** offsets, const uint32_t** table) {
     if (!c) return fail(c, GSJ_ERR_INVALID, "null context");
     if (!c->have_result) return fail(c, GSJ_ERR_STATE, "no join result");
+    if (table && !c->table_on_device) return fail(c, GSJ_ERR_STATE, "the last join delivered its table to host memory");
     if (counts) *counts = static_cast<const uint32_t*>(c->counts.p);
     if (offsets) *offsets = static_cast<const uint64_t*>(c->offsets.p);
     if (table) *table = static_cast<const uint32_t*>(c->table.p);
@@ -1218,6 +1519,141 @@ const char* gsj_last_error(gsj_context* c) {
 
 float gsj_threshold_f32(float eps) { return threshold_of<float>(eps); }
 double gsj_threshold_f64(double eps) { return threshold_of<double>(eps); }
+
+// ---------------------------------------------------------------- learned model
+static int model_ensure(gsj_context* c) {
+    float *w = nullptr, *m1 = nullptr, *m2 = nullptr;
+    GSJ_TRY(dev_get(c, c->mw, kModelWeights, &w));
+    GSJ_TRY(dev_get(c, c->mm1, kModelWeights, &m1));
+    GSJ_TRY(dev_get(c, c->mm2, kModelWeights, &m2));
+    if (!c->model_ready) {
+        GSJ_CUDA(c, model_init(w, m1, m2, 0x5eed1234u, c->st));
+        c->model_ready = true;
+        c->model_trained = false;
+        c->model_t = 0;
+        c->model_unc_ratio = 0.0;
+    }
+    return GSJ_OK;
+}
+
+// Features and targets of the last join's cells into c->mx / c->my.
+static int model_dataset(gsj_context* c, uint32_t* M_out) {
+    if (!c->have_result || !c->last.valid) return fail(c, GSJ_ERR_STATE, "no indexed join result to learn from");
+    const uint32_t M = c->last.M;
+    float *X = nullptr, *Y = nullptr;
+    GSJ_TRY(dev_get(c, c->mx, (size_t)M * kModelFeatures, &X));
+    GSJ_TRY(dev_get(c, c->my, M, &Y));
+    GSJ_CUDA(c, model_features(c->last.lookup, M, c->last.log2_eps, c->last.n, X, c->st));
+    GSJ_CUDA(c, model_targets(c->last.lookup.cell_start, c->last.lookup.ids, static_cast<const uint32_t*>(c->counts.p),
+                              M, Y, c->st));
+    *M_out = M;
+    return GSJ_OK;
+}
+
+int gsj_model_reset(gsj_context* c) {
+    if (!c) return fail(c, GSJ_ERR_INVALID, "null context");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    c->model_ready = false;
+    GSJ_TRY(model_ensure(c));
+    GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+    return GSJ_OK;
+}
+
+int gsj_model_train(gsj_context* c, uint32_t steps, float* loss) {
+    if (!c) return fail(c, GSJ_ERR_INVALID, "null context");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    GSJ_TRY(model_ensure(c));
+    uint32_t M = 0;
+    GSJ_TRY(model_dataset(c, &M));
+    if (M == 0) return fail(c, GSJ_ERR_STATE, "the last join has no cells");
+    const uint32_t ntr = std::min<uint32_t>(M, kModelTrainRows);
+    float *Xt = nullptr, *Yt = nullptr, *d_loss = nullptr;
+    GSJ_TRY(dev_get(c, c->mxt, (size_t)ntr * kModelFeatures, &Xt));
+    GSJ_TRY(dev_get(c, c->myt, ntr, &Yt));
+    GSJ_TRY(dev_get(c, c->mtmp, 4, reinterpret_cast<double**>(&d_loss)));
+    GSJ_CUDA(c, model_subsample(static_cast<const float*>(c->mx.p), static_cast<const float*>(c->my.p), M, ntr, Xt,
+                                Yt, c->st));
+    GSJ_CUDA(c, model_train(Xt, Yt, ntr, static_cast<float*>(c->mw.p), static_cast<float*>(c->mm1.p),
+                            static_cast<float*>(c->mm2.p), c->model_t, steps, 3e-3f, d_loss + 2, c->st));
+    c->model_t += steps;
+    float l = 0.f;
+    GSJ_TRY(d2h_small(c, &l, d_loss + 2, 1));
+    if (loss) *loss = l;
+    c->model_trained = steps > 0 || c->model_trained;
+    if (c->stats.join_path == GSJ_PATH_SCREEN && c->stats.total_pairs)
+        c->model_unc_ratio = (double)c->stats.screen_rechecks / (double)c->stats.total_pairs;
+    return GSJ_OK;
+}
+
+int gsj_model_weights(gsj_context* c, float* weights, uint32_t count, int set) {
+    if (!c || !weights) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (count != (uint32_t)kModelWeights)
+        return fail(c, GSJ_ERR_INVALID, "the model has " + std::to_string(kModelWeights) + " weights");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    GSJ_TRY(model_ensure(c));
+    if (set) {
+        GSJ_CUDA(c, cudaMemcpyAsync(c->mw.p, weights, count * sizeof(float), cudaMemcpyHostToDevice, c->st));
+        GSJ_CUDA(c, cudaMemsetAsync(c->mm1.p, 0, count * sizeof(float), c->st));
+        GSJ_CUDA(c, cudaMemsetAsync(c->mm2.p, 0, count * sizeof(float), c->st));
+        GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+        c->model_t = 0;
+        c->model_trained = true;
+        return GSJ_OK;
+    }
+    return d2h_small(c, weights, static_cast<const float*>(c->mw.p), count);
+}
+
+int gsj_model_features(gsj_context* c, float* features, float* targets, uint32_t cap, uint32_t* cells) {
+    if (!c || !cells) return fail(c, GSJ_ERR_INVALID, "null argument");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    uint32_t M = 0;
+    GSJ_TRY(model_dataset(c, &M));
+    *cells = M;
+    if (cap < M) {
+        GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+        return GSJ_OK;
+    }
+    if (features) GSJ_TRY(d2h_small(c, features, static_cast<const float*>(c->mx.p), (size_t)M * kModelFeatures));
+    if (targets) GSJ_TRY(d2h_small(c, targets, static_cast<const float*>(c->my.p), M));
+    GSJ_CUDA(c, cudaStreamSynchronize(c->st));
+    return GSJ_OK;
+}
+
+// Host rows -> device scratch (c->mxt / c->myt).
+static int model_upload(gsj_context* c, const float* features, const float* targets, uint32_t n, float** X,
+                        float** Y) {
+    GSJ_TRY(dev_get(c, c->mxt, (size_t)n * kModelFeatures, X));
+    GSJ_TRY(dev_get(c, c->myt, n, Y));
+    GSJ_CUDA(c, cudaMemcpyAsync(*X, features, (size_t)n * kModelFeatures * sizeof(float), cudaMemcpyHostToDevice,
+                                c->st));
+    if (targets) GSJ_CUDA(c, cudaMemcpyAsync(*Y, targets, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    return GSJ_OK;
+}
+
+int gsj_model_predict(gsj_context* c, const float* features, uint32_t n, float* out) {
+    if (!c || (n && (!features || !out))) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (n == 0) return GSJ_OK;
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    GSJ_TRY(model_ensure(c));
+    float *X = nullptr, *Y = nullptr;
+    GSJ_TRY(model_upload(c, features, nullptr, n, &X, &Y));
+    GSJ_CUDA(c, model_predict(X, n, static_cast<const float*>(c->mw.p), Y, nullptr, 0.f, nullptr, c->st));
+    return d2h_small(c, out, Y, n);
+}
+
+int gsj_model_loss_grad(gsj_context* c, const float* features, const float* targets, uint32_t n, float* loss,
+                        float* grad) {
+    if (!c || !features || !targets || !loss || !grad) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (n == 0) return fail(c, GSJ_ERR_INVALID, "no rows");
+    GSJ_CUDA(c, cudaSetDevice(c->device));
+    GSJ_TRY(model_ensure(c));
+    float *X = nullptr, *Y = nullptr, *g = nullptr;
+    GSJ_TRY(model_upload(c, features, targets, n, &X, &Y));
+    GSJ_TRY(dev_get(c, c->mtmp, kModelWeights + 8, reinterpret_cast<double**>(&g)));
+    GSJ_CUDA(c, model_grad(X, Y, n, static_cast<const float*>(c->mw.p), g + kModelWeights, g, c->st));
+    GSJ_TRY(d2h_small(c, loss, g + kModelWeights, 1));
+    return d2h_small(c, grad, g, kModelWeights);
+}
 
 // ---------------------------------------------------------------- drop-in
 static std::mutex g_py_mu;

@@ -34,6 +34,10 @@ class JoinConfig:
     no_unicomp: bool = False  # full-neighbourhood traversal even with stamp (same pair set)
     plain: bool = False       # no tensor-core screen (every pair in exact FP32; same pair set)
     exact_size: bool = False  # pair buffers sized by a counting pass, not an estimate (same pair set)
+    buffer_pairs: int = 0     # GPUBUFFERSIZE: entries per device result segment of run_host (0: 100M)
+    streams: int = 0          # GPUSTREAMS: result segments in flight in run_host (0: 3)
+    min_batches: int = 0      # MINBATCHES: fewest result batches of run_host (0: 3)
+    learned: bool = False     # size pair buffers with the context's learned result-count model
 
 
 class SelfJoin:
@@ -76,6 +80,10 @@ class SelfJoin:
         c.flags = (N.GSJ_FLAG_QUIET | (N.GSJ_FLAG_SORT_LISTS if cfg.sort_lists else 0)
                    | (N.GSJ_FLAG_NO_UNICOMP if cfg.no_unicomp else 0) | (N.GSJ_FLAG_PLAIN if cfg.plain else 0)
                    | (N.GSJ_FLAG_EXACT_SIZE if cfg.exact_size else 0))
+        c.buffer_pairs = int(cfg.buffer_pairs)
+        c.streams = int(cfg.streams)
+        c.min_batches = int(cfg.min_batches)
+        c.estimator = N.GSJ_EST_LEARNED if cfg.learned else N.GSJ_EST_SAMPLED
         return c
 
     def run(self, points, eps: float, config: JoinConfig | None = None, **kw) -> dict:
@@ -106,6 +114,91 @@ class SelfJoin:
                     self._ctx)
         self.N, self.n = Np, n
         return st.as_dict()
+
+    def run_host(self, points, eps: float, config: JoinConfig | None = None, counts: np.ndarray | None = None,
+                 table: np.ndarray | None = None, **kw) -> tuple[dict, np.ndarray, np.ndarray]:
+        """Runs the join with the result delivered to host memory
+        (gsj_join_host): the table is produced in batches that are copied to
+        the host while the next batch is computed.  ``counts``/``table`` may
+        be given (pinned buffers are written by DMA directly); a table that is
+        too small is replaced by one of the exact size and the join repeated.
+        Returns (stats, numNeighbors, neighborTable)."""
+        cfg = config or JoinConfig(**kw)
+        st = N.GsjStats()
+        on_dev = hasattr(points, "is_cuda") and points.is_cuda
+        if on_dev:
+            Np, n = points.shape
+            import torch
+
+            dt = np.float64 if points.dtype == torch.float64 else np.float32
+            ptr = ctypes.c_void_p(points.data_ptr())
+        else:
+            p = np.ascontiguousarray(points)
+            if p.dtype not in (np.float32, np.float64):
+                p = p.astype(np.float32)
+            Np, n = p.shape
+            dt = p.dtype
+            ptr = ctypes.c_void_p(p.ctypes.data)
+        c = self._cfg(n, dt, cfg)
+        counts = np.empty(Np, dtype=np.uint32) if counts is None else counts
+        table = np.empty(0, dtype=np.uint32) if table is None else table
+        total = ctypes.c_uint64()
+        for _ in range(2):
+            rc = self._L.gsj_join_host(self._ctx, ptr, Np, float(eps), ctypes.byref(c), int(on_dev),
+                                       counts.ctypes.data, table.ctypes.data if table.size else None, table.size,
+                                       ctypes.byref(total), ctypes.byref(st))
+            if rc == N.GSJ_ERR_OVERFLOW:
+                table = np.empty(int(total.value), dtype=np.uint32)
+                continue
+            N.check(rc, self._ctx)
+            break
+        self.N, self.n = Np, n
+        return st.as_dict(), counts, table[: int(total.value)]
+
+    # ---- learned result-count model (GSJ_EST_LEARNED)
+    def model_train(self, steps: int = 400) -> float:
+        """Trains the context's model on the exact counts of the last join;
+        returns the last minibatch loss."""
+        loss = ctypes.c_float()
+        N.check(self._L.gsj_model_train(self._ctx, int(steps), ctypes.byref(loss)), self._ctx)
+        return float(loss.value)
+
+    def model_reset(self) -> None:
+        N.check(self._L.gsj_model_reset(self._ctx), self._ctx)
+
+    def model_weights(self, weights: np.ndarray | None = None) -> np.ndarray:
+        """The model's weights; with `weights`, sets them first."""
+        if weights is not None:
+            w = np.ascontiguousarray(weights, dtype=np.float32)
+            N.check(self._L.gsj_model_weights(self._ctx, w.ctypes.data, w.size, 1), self._ctx)
+        out = np.empty(N.MODEL_WEIGHTS, dtype=np.float32)
+        N.check(self._L.gsj_model_weights(self._ctx, out.ctypes.data, out.size, 0), self._ctx)
+        return out
+
+    def model_features(self) -> tuple[np.ndarray, np.ndarray]:
+        """The last join's per-cell features and targets (log2(1 + mean count))."""
+        m = ctypes.c_uint32()
+        N.check(self._L.gsj_model_features(self._ctx, None, None, 0, ctypes.byref(m)), self._ctx)
+        X = np.empty((m.value, N.MODEL_FEATURES), dtype=np.float32)
+        y = np.empty(m.value, dtype=np.float32)
+        N.check(self._L.gsj_model_features(self._ctx, X.ctypes.data, y.ctypes.data, m.value, ctypes.byref(m)),
+                self._ctx)
+        return X, y
+
+    def model_predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.empty(X.shape[0], dtype=np.float32)
+        N.check(self._L.gsj_model_predict(self._ctx, X.ctypes.data, X.shape[0], out.ctypes.data), self._ctx)
+        return out
+
+    def model_loss_grad(self, X: np.ndarray, y: np.ndarray) -> tuple[float, np.ndarray]:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        grad = np.empty(N.MODEL_WEIGHTS, dtype=np.float32)
+        N.check(self._L.gsj_model_loss_grad(self._ctx, X.ctypes.data, y.ctypes.data, X.shape[0], loss.ctypes.data,
+                                            grad.ctypes.data), self._ctx)
+        return float(loss[0]), grad
 
     def bruteforce(self, points, eps: float) -> tuple[np.ndarray, int]:
         """Brute-force neighbour counts over all N^2 pairs (the reference's GPU

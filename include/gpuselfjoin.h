@@ -75,7 +75,26 @@ typedef struct gsj_config {
     uint32_t query_reorder; /* QUERYREORDER   schedule heavy query cells first   */
     int32_t device;         /* gpuContext     CUDA device ordinal                */
     uint32_t flags;         /* GSJ_FLAG_*                                        */
+    /* Batching scheme (params.h:78-93), used when results go to host memory
+     * (gsj_join_host): the table is produced in batches of point ids whose
+     * lists fit one device result segment, each copied to the host while the
+     * next is computed. */
+    uint64_t buffer_pairs;  /* GPUBUFFERSIZE  result entries per device segment
+                                              (0: 100,000,000)                   */
+    uint32_t streams;       /* GPUSTREAMS     segments in flight (0: 3)          */
+    uint32_t min_batches;   /* MINBATCHES     fewest batches (0: 3)              */
+    uint32_t estimator;     /* GSJ_EST_*      result-size estimate of the pair
+                                              paths (SAMPLERATE's role)         */
+    uint32_t reserved;      /* zero                                             */
 } gsj_config;
+
+/* Result-size estimators (gsj_config.estimator): how the warp, tile and screen
+ * paths size their pair buffers before the exact pass (a short buffer is
+ * re-sized and the pass repeated, so the output never depends on it). */
+#define GSJ_EST_SAMPLED 0u /* an exact pass over every 64th work item         */
+#define GSJ_EST_LEARNED 1u /* the context's result-count model (gsj_model_*),
+                              trained on the counts of earlier joins; the sampled
+                              estimate while the model is untrained          */
 
 /* Statistics of the most recent join of a context. */
 typedef struct gsj_stats {
@@ -102,6 +121,10 @@ typedef struct gsj_stats {
                                  reject, evaluated exactly (0 on other paths)   */
     uint64_t reruns;          /* passes repeated because a buffer sized from the
                                  estimate was short (the output is unchanged)  */
+    uint64_t batches;         /* result batches of gsj_join_host (1 otherwise)  */
+    uint64_t estimate;        /* pairs (or undecided pairs) the estimator
+                                 predicted for the exact pass                  */
+    double dev_ms_estimate;   /* device time of the estimate                    */
 } gsj_stats;
 
 /* Join paths (gsj_stats.join_path). */
@@ -137,6 +160,24 @@ GSJ_API int gsj_destroy(gsj_context* ctx);
  */
 GSJ_API int gsj_join(gsj_context* ctx, const void* data, uint64_t num_points, double eps,
              const gsj_config* cfg, int data_on_device, gsj_stats* stats);
+
+/*
+ * Runs the self-join and delivers the result to host memory: numNeighbors into
+ * num_neighbors[N] (host) and neighborTable into neighbor_table (host, `cap`
+ * entries).  Replaces distanceTableNDGridBatches' batch loop (GPU.cu:765-994)
+ * with a pipeline: on the dense low-dimensional path the table is produced in
+ * batches of point ids whose lists fit one device segment of
+ * cfg->buffer_pairs entries, and each batch is copied to the host (directly
+ * into pinned destinations, through pinned staging otherwise) while the next
+ * one is computed, cfg->streams segments in flight; the other paths copy the
+ * finished table.  When cap < R, *total_pairs receives R, num_neighbors is
+ * filled, no table entry is written and GSJ_ERR_OVERFLOW is returned.  The
+ * device keeps numNeighbors and the offsets (gsj_result_device) but not
+ * necessarily the table afterwards.
+ */
+GSJ_API int gsj_join_host(gsj_context* ctx, const void* data, uint64_t num_points, double eps,
+                          const gsj_config* cfg, int data_on_device, uint32_t* num_neighbors,
+                          uint32_t* neighbor_table, uint64_t cap, uint64_t* total_pairs, gsj_stats* stats);
 
 /* Number of result pairs R of the last join. */
 GSJ_API int gsj_result_size(gsj_context* ctx, uint64_t* total_pairs);
@@ -202,6 +243,37 @@ GSJ_API int gsj_bruteforce_count(gsj_context* ctx, const void* data, uint64_t nu
  * the caller.
  */
 GSJ_API int gsj_list_offsets_noalloc(const uint32_t* d_counts, uint64_t n, uint64_t* d_offsets, void* stream);
+
+/* ---------------------------------------------------------------- learned
+ * The context's result-count model (GSJ_EST_LEARNED): a 16-64-32-1 MLP
+ * (GSJ_MODEL_WEIGHTS weights) that predicts the mean neighbour count of a
+ * cell's queries from the sizes of the cell and its face-adjacent cells, eps
+ * and the dimensionality.  It replaces the reference's sampled estimator
+ * (callGPUBatchEst, GPU.cu:57-268; SAMPLERATE, params.h:93) for sizing the
+ * pair buffers; the exact count still judges every buffer.  Training and
+ * inference run on the device with this library's own kernels. */
+#define GSJ_MODEL_WEIGHTS 3201
+#define GSJ_MODEL_FEATURES 16
+
+/* Trains the model for `steps` Adam steps on the exact per-cell counts of the
+ * last join of ctx (up to 65,536 of its cells); *loss (optional) receives the
+ * last minibatch's mean squared error of log2(1 + count). */
+GSJ_API int gsj_model_train(gsj_context* ctx, uint32_t steps, float* loss);
+/* Back to the initial (untrained) weights. */
+GSJ_API int gsj_model_reset(gsj_context* ctx);
+/* Copies the weights out (set == 0) or in (set != 0; marks the model
+ * trained); count must be GSJ_MODEL_WEIGHTS. */
+GSJ_API int gsj_model_weights(gsj_context* ctx, float* weights, uint32_t count, int set);
+/* The last join's per-cell features [cells][GSJ_MODEL_FEATURES] and targets
+ * [cells] (host arrays of capacity `cap` rows; only *cells is written when
+ * cap is smaller). */
+GSJ_API int gsj_model_features(gsj_context* ctx, float* features, float* targets, uint32_t cap, uint32_t* cells);
+/* Network outputs (log2(1 + count)) of n host feature rows. */
+GSJ_API int gsj_model_predict(gsj_context* ctx, const float* features, uint32_t n, float* out);
+/* Mean squared error over n host rows and its gradient (GSJ_MODEL_WEIGHTS
+ * floats), computed by the training kernels' forward and backward code. */
+GSJ_API int gsj_model_loss_grad(gsj_context* ctx, const float* features, const float* targets, uint32_t n,
+                                float* loss, float* grad);
 
 /* ---------------------------------------------------------------- drop-in
  * The reference's shared-library ABI (built with -DPYTHON, Makefile:58-77).
