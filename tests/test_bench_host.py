@@ -16,22 +16,25 @@ def _stats(path, count_ms, fill_ms, candidates=0):
 
 def test_rows_path_fill_dominant():
     w = synth.WORKLOADS["c2_gmm2d"]
-    N, n, R = w.N, w.n, 642_337_374
-    roof = bench._roofline(_stats(1, 1.4, 5.2), N, n, R, w)
+    N, n, R, C = w.N, w.n, 642_337_374, 1_802_646_654
+    roof = bench._roofline(_stats(1, 1.4, 5.2, C), N, n, R, w)
     assert roof["kernel"] == "join_fill" and roof["bound"] == "hbm" and roof["unit"] == "GB/s"
-    want = 4.0 * N * n + 4.0 * N + 8.0 * N + 4.0 * R
+    want = 4.0 * R + 24.0 * N + C / 8.0  # table, per-query metadata, hit masks
     assert roof["algorithmic_bytes"] == want
     assert math.isclose(roof["achieved"], want / 5.2e-3 / 1e9)
     assert math.isclose(roof["frac"], roof["achieved"] / roof["peak"])
-    # the committed ncu summary for this kernel and workload carries its DRAM bytes
-    assert roof["traffic"] is not None and roof["traffic"] > want
+    # the whole join against the path's algorithmic bytes 4Nn + 4N + 4R
+    b_alg = 4.0 * N * n + 4.0 * N + 4.0 * R
+    assert roof["join"]["algorithmic_bytes"] == b_alg
+    assert math.isclose(roof["join"]["ms"], 1.0 + 1.4 + 5.2)
 
 
-def test_rows_path_count_dominant_with_stamp():
+def test_rows_path_count_dominant():
     w = synth.WORKLOADS["c2_gmm2d"]
-    roof = bench._roofline(_stats(1, 6.0, 5.0), w.N, w.n, 10, w)
+    C = 1_000_000
+    roof = bench._roofline(_stats(1, 6.0, 5.0, C), w.N, w.n, 10, w)
     assert roof["kernel"] == "join_count"
-    assert roof["algorithmic_bytes"] == 4.0 * w.N * w.n + 4.0 * w.N * 3  # STAMP: reverse counts too
+    assert roof["algorithmic_bytes"] == 4.0 * w.N * w.n + 4.0 * w.N + 8.0 * w.N + C / 8.0
 
 
 @pytest.mark.parametrize("path", [0, 2])
@@ -41,9 +44,9 @@ def test_emit_paths(path):
     roof = bench._roofline(_stats(path, 38.4, 19.9), w.N, w.n, R, w)
     assert roof["kernel"] == "join_emit" and roof["bound"] == "hbm"
     assert roof["algorithmic_bytes"] == 4.0 * w.N * w.n + 4.0 * w.N + 8.0 * R
-    sort = bench._roofline(_stats(path, 10.0, 19.9), w.N, w.n, R, w)
-    assert sort["kernel"] == "pair_sort"
-    assert sort["algorithmic_bytes"] == 12.0 * R + 8.0 * w.N
+    place = bench._roofline(_stats(path, 10.0, 19.9), w.N, w.n, R, w)
+    assert place["kernel"] == "pair_place"
+    assert place["algorithmic_bytes"] == 12.0 * R + 8.0 * w.N
 
 
 def test_screen_path_is_a_tensor_roofline():
