@@ -708,6 +708,8 @@ int rows_to_host(gsj_context* c, JoinArgs<T>& a, const gsj_config& cfg, uint64_t
     uint64_t step = seg_cap - lmax;
     const uint64_t even = (R + min_b - 1) / min_b;
     if (even >= 1 && even < step) step = even;
+    // a batch holds fewer than step + lmax entries: no segment needs more
+    seg_cap = std::min<uint64_t>(seg_cap, step + lmax);
     const uint64_t nb64 = R ? (R + step - 1) / step : 1;
     if (nb64 > 65535) return fail(c, GSJ_ERR_INVALID, "more than 65535 result batches: raise buffer_pairs");
     const uint32_t nb = (uint32_t)nb64;
@@ -755,6 +757,7 @@ int rows_to_host(gsj_context* c, JoinArgs<T>& a, const gsj_config& cfg, uint64_t
     GSJ_TRY(dev_get(c, c->segs, (size_t)nseg * seg_cap, &segs));
     if (!table_pinned)
         for (int i = 0; i < nseg; i++) GSJ_TRY(pinned_get(c, c->hseg[i], seg_cap * sizeof(uint32_t)));
+    a.offsets = offsets;
     a.table_cap = seg_cap;
     a.err_flag = ctr + 1;
     GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
