@@ -13,18 +13,19 @@
 //                 reference's arithmetic and records the decisions as a bit
 //                 mask (bit f of the query's words), the list length by slot and
 //                 by point id.
-//   k_rows_fill   a warp per 32 consecutive query slots.  Each lane replays its
-//                 query's bit mask - no second distance pass - and writes the
-//                 hit ids to the warp's shared-memory stage at the query's
-//                 position within the warp's 32 lists; the warp then stores the
-//                 32 lists to their places in the point-id-ordered table, each
-//                 list with consecutive lanes.  A warp whose lists exceed the
-//                 stage is done in several windows.
+//   k_rows_fill   a warp per 32 consecutive query slots, the queries taken one
+//                 after another.  The warp replays the query's bit mask - no
+//                 second distance pass - 32 candidates per mask word: lane j
+//                 takes bit j, loads the id of its candidate when the bit is set,
+//                 and stores it at the query's next free list position, so each
+//                 word's hits are written by consecutive lanes to consecutive
+//                 places of the point-id-ordered table.
 // Both kernels claim their 32-slot chunks dynamically (one atomic per warp,
 // the next claim issued before the current chunk is processed), since chunk
 // costs vary with the local density by orders of magnitude.
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <type_traits>
 
 #include "gsj_common.cuh"
 #include "gsj_dist.cuh"
@@ -44,6 +45,35 @@ __device__ __forceinline__ uint32_t claim32(uint32_t* ctr, int lane) {
 
 }  // namespace
 
+// Coordinates of one point row (NT values of a row padded to npad = 1, 2 or
+// 4 entries, so the vector forms are aligned).
+template <typename T, int NT>
+__device__ __forceinline__ void load_row(const T* __restrict__ p, T (&r)[NT]) {
+    if constexpr (std::is_same<T, float>::value && NT == 2) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        r[0] = v.x;
+        r[1] = v.y;
+    } else if constexpr (std::is_same<T, float>::value && NT >= 3) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        r[0] = v.x;
+        r[1] = v.y;
+        r[2] = v.z;
+        if constexpr (NT == 4) r[3] = v.w;
+    } else if constexpr (std::is_same<T, double>::value && NT >= 2) {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        r[0] = v.x;
+        r[1] = v.y;
+        if constexpr (NT >= 3) {
+            const double2 w = *reinterpret_cast<const double2*>(p + 2);
+            r[2] = w.x;
+            if constexpr (NT == 4) r[3] = w.y;
+        }
+    } else {
+#pragma unroll
+        for (int l = 0; l < NT; l++) r[l] = p[l];
+    }
+}
+
 template <typename T, int NT, int NR, int POL>
 __global__ void __launch_bounds__(256) k_rows_count(const JoinArgs<T> a, const uint32_t* __restrict__ slot_cell,
                                                     const uint64_t* __restrict__ bitoff, uint32_t* __restrict__ bits,
@@ -52,6 +82,7 @@ __global__ void __launch_bounds__(256) k_rows_count(const JoinArgs<T> a, const u
     const int lane = threadIdx.x & 31;
     const uint32_t N = a.n_points;
     const uint32_t npad = a.npad;
+    const T thr = a.thr;
     unsigned long long cand = 0;
     uint32_t cur = __shfl_sync(FULL, claim32(a.work_counter, lane), 0);
     while (cur < N) {
@@ -60,33 +91,42 @@ __global__ void __launch_bounds__(256) k_rows_count(const JoinArgs<T> a, const u
         if (s < N) {
             const uint32_t cell = slot_cell[s];
             T q[NT];
-#pragma unroll
-            for (int l = 0; l < NT; l++) q[l] = a.pts[(size_t)s * npad + l];
+            load_row<T, NT>(a.pts + (size_t)s * npad, q);
             uint64_t wp = bitoff[s];
-            uint32_t cnt = 0, word = 0, f = 0;
+            uint32_t cnt = 0, word = 0, b = 0;  // b: next bit of the current mask word
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 const uint2 e = a.plan[(size_t)cell * NR + r];
-                for (uint32_t i = 0; i < e.y; i++) {
-                    const uint32_t c = e.x + i;
-                    T cr[NT];
-#pragma unroll
-                    for (int l = 0; l < NT; l++) cr[l] = a.pts[(size_t)c * npad + l];
-                    const T d2 = sqdist_seq_reg<T, NT, POL>(q, cr);
-                    const uint32_t hit = d2 <= a.thr ? 1u : 0u;
-                    word |= hit << (f & 31u);
-                    cnt += hit;
-                    f++;
-                    if ((f & 31u) == 0u) {
+                const T* cp = a.pts + (size_t)e.x * npad;
+                uint32_t left = e.y;
+                cand += left;
+                while (left) {
+                    // candidates up to the end of the current mask word
+                    const uint32_t m = min(left, 32u - b);
+#pragma unroll 4
+                    for (uint32_t u = 0; u < m; u++) {
+                        T cr[NT];
+                        load_row<T, NT>(cp, cr);
+                        cp += npad;
+                        const T d2 = sqdist_seq_reg<T, NT, POL>(q, cr);
+                        word |= (d2 <= thr ? 1u : 0u) << (b + u);
+                    }
+                    b += m;
+                    left -= m;
+                    if (b == 32u) {
                         bits[wp++] = word;
+                        cnt += (uint32_t)__popc(word);
                         word = 0u;
+                        b = 0u;
                     }
                 }
             }
-            if (f & 31u) bits[wp] = word;
+            if (b) {
+                bits[wp] = word;
+                cnt += (uint32_t)__popc(word);
+            }
             a.fwd_cnt[s] = cnt;
             counts_by_id[a.ids[s]] = cnt;
-            cand += f;
         }
         cur = __shfl_sync(FULL, nxt, 0);
     }
@@ -95,30 +135,36 @@ __global__ void __launch_bounds__(256) k_rows_count(const JoinArgs<T> a, const u
     if (lane == 0 && cand) atomicAdd(a.cand_cnt, cand);
 }
 
+__device__ __forceinline__ unsigned lanemask_lt_q() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
 // Queries: the slots qslots[0 .. nq) (all slots 0 .. nq-1 when qslots is
 // null); the list of point id i goes to a.table[offsets[i] - base].
-template <int NR, int CAP>
-__global__ void __launch_bounds__(128) k_rows_fill(const JoinArgs<float> a, const uint32_t* __restrict__ slot_cell,
+template <int NR>
+__global__ void __launch_bounds__(256) k_rows_fill(const JoinArgs<float> a, const uint32_t* __restrict__ slot_cell,
                                                    const uint64_t* __restrict__ bitoff,
                                                    const uint32_t* __restrict__ bits,
                                                    const uint32_t* __restrict__ qslots, uint32_t nq, uint64_t base) {
-    __shared__ uint32_t stage_all[4][CAP];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    uint32_t* stage = stage_all[threadIdx.x >> 5];
+    const unsigned lt = lanemask_lt_q();
     uint32_t cur = __shfl_sync(FULL, claim32(a.work_counter, lane), 0);
     while (cur < nq) {
         const uint32_t nxt = claim32(a.work_counter, lane);
         const uint32_t j = cur + (uint32_t)lane;
-        const bool valid = j < nq;
-        const uint32_t s = valid ? (qslots ? qslots[j] : j) : 0u;
+        const uint32_t nv = min(32u, nq - cur);
+        // lane j: query j's list length, mask words, list place and candidate rows
         uint32_t cnt = 0, nw = 0;
         uint64_t bo = 0;
         unsigned long long dst = 0;
         uint32_t lo[NR], pre[NR];
 #pragma unroll
         for (int r = 0; r < NR; r++) lo[r] = pre[r] = 0u;
-        if (valid) {
+        if (j < nq) {
+            const uint32_t s = qslots ? qslots[j] : j;
             cnt = a.fwd_cnt[s];
             bo = bitoff[s];
             nw = (uint32_t)(bitoff[s + 1] - bo);
@@ -137,52 +183,37 @@ __global__ void __launch_bounds__(128) k_rows_fill(const JoinArgs<float> a, cons
                 p += e.y;
             }
         }
-        // position of this lane's list among the warp's 32 lists
-        uint32_t x = cnt;
+        for (uint32_t qi = 0; qi < nv; qi++) {
+            const uint32_t cq = __shfl_sync(FULL, cnt, qi);
+            if (cq == 0u) continue;
+            const unsigned long long dq = __shfl_sync(FULL, dst, qi);
+            const unsigned long long bq = __shfl_sync(FULL, bo, qi);
+            const uint32_t nwq = __shfl_sync(FULL, nw, qi);
+            uint32_t lq[NR], pq[NR];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(FULL, x, o);
-            if (lane >= o) x += y;
-        }
-        const uint32_t total = __shfl_sync(FULL, x, 31);
-        const uint32_t my_off = x - cnt;
-        for (uint32_t w0 = 0; w0 < total; w0 += (uint32_t)CAP) {
-            const uint32_t w1 = w0 + (uint32_t)CAP;
-            if (cnt && my_off < w1 && my_off + cnt > w0) {
-                uint32_t k = my_off;  // position of the next hit
-                for (uint32_t t = 0; t < nw && k < w1; t++) {
-                    uint32_t word = bits[bo + t];
-                    const uint32_t pc = (uint32_t)__popc(word);
-                    if (k + pc <= w0) {
-                        k += pc;
-                        continue;
-                    }
-                    while (word) {
-                        const uint32_t b = (uint32_t)(__ffs(word) - 1);
-                        word &= word - 1u;
-                        if (k >= w0 && k < w1) {
-                            const uint32_t f = t * 32u + b;
-                            uint32_t st = lo[0] + f;
+            for (int r = 0; r < NR; r++) {
+                lq[r] = __shfl_sync(FULL, lo[r], qi);
+                pq[r] = __shfl_sync(FULL, pre[r], qi);
+            }
+            uint32_t* list = a.table + dq;
+            uint32_t run = 0;  // entries of the list written so far
+            for (uint32_t t0 = 0; t0 < nwq && run < cq; t0 += 32u) {
+                const uint32_t myw = (t0 + (uint32_t)lane < nwq) ? bits[bq + t0 + lane] : 0u;
+                const uint32_t tn = min(32u, nwq - t0);
+                for (uint32_t tt = 0; tt < tn; tt++) {
+                    const uint32_t word = __shfl_sync(FULL, myw, tt);
+                    if (word == 0u) continue;
+                    if ((word >> lane) & 1u) {
+                        const uint32_t f = (t0 + tt) * 32u + (uint32_t)lane;
+                        uint32_t st = lq[0] + f;
 #pragma unroll
-                            for (int r = 1; r < NR; r++)
-                                if (f >= pre[r]) st = lo[r] + (f - pre[r]);
-                            stage[k - w0] = a.ids[st];
-                        }
-                        k++;
+                        for (int r = 1; r < NR; r++)
+                            if (f >= pq[r]) st = lq[r] + (f - pq[r]);
+                        list[run + (uint32_t)__popc(word & lt)] = a.ids[st];
                     }
+                    run += (uint32_t)__popc(word);
                 }
             }
-            __syncwarp();
-            // the warp stores the window's part of each list with consecutive lanes
-            for (int jj = 0; jj < 32; jj++) {
-                const uint32_t oj = __shfl_sync(FULL, my_off, jj);
-                const uint32_t cj = __shfl_sync(FULL, cnt, jj);
-                const unsigned long long dj = __shfl_sync(FULL, dst, jj);
-                const uint32_t b0 = oj > w0 ? oj : w0;
-                const uint32_t e0 = (oj + cj) < w1 ? (oj + cj) : w1;
-                for (uint32_t p = b0 + (uint32_t)lane; p < e0; p += 32u) a.table[dj + (p - oj)] = stage[p - w0];
-            }
-            __syncwarp();
         }
         cur = __shfl_sync(FULL, nxt, 0);
     }
@@ -233,18 +264,16 @@ cudaError_t launch_rows_count(const JoinArgs<T>& a, const uint32_t* slot_cell, c
     return count_nr<T, 9>(a, slot_cell, bitoff, bits, counts_by_id, num_sms, st);
 }
 
-constexpr int kFillCap = 2048;  // stage entries per warp (8 KB)
-
 template <int NR>
 static cudaError_t fill_nr(const JoinArgs<float>& a, const uint32_t* slot_cell, const uint64_t* bitoff,
                            const uint32_t* bits, const uint32_t* qslots, uint32_t nq, uint64_t base, int num_sms,
                            cudaStream_t st) {
     if (nq == 0) return cudaSuccess;
-    auto kern = k_rows_fill<NR, kFillCap>;
-    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, 128, 0, num_sms);
-    const uint64_t needed = ((uint64_t)nq + 127) / 128;
+    auto kern = k_rows_fill<NR>;
+    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, 256, 0, num_sms);
+    const uint64_t needed = ((uint64_t)nq + 255) / 256;
     if (blocks > needed) blocks = needed ? needed : 1;
-    kern<<<(unsigned)blocks, 128, 0, st>>>(a, slot_cell, bitoff, bits, qslots, nq, base);
+    kern<<<(unsigned)blocks, 256, 0, st>>>(a, slot_cell, bitoff, bits, qslots, nq, base);
     return cudaGetLastError();
 }
 
