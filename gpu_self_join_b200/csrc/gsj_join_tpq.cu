@@ -200,18 +200,30 @@ __global__ void __launch_bounds__(256) k_rows_fill(const JoinArgs<float> a, cons
             for (uint32_t t0 = 0; t0 < nwq && run < cq; t0 += 32u) {
                 const uint32_t myw = (t0 + (uint32_t)lane < nwq) ? bits[bq + t0 + lane] : 0u;
                 const uint32_t tn = min(32u, nwq - t0);
-                for (uint32_t tt = 0; tt < tn; tt++) {
-                    const uint32_t word = __shfl_sync(FULL, myw, tt);
-                    if (word == 0u) continue;
-                    if ((word >> lane) & 1u) {
-                        const uint32_t f = (t0 + tt) * 32u + (uint32_t)lane;
-                        uint32_t st = lq[0] + f;
+                // two mask words (64 candidates) per step
+                for (uint32_t tt = 0; tt < tn; tt += 2u) {
+                    const uint32_t w0 = __shfl_sync(FULL, myw, tt);
+                    uint32_t w1 = __shfl_sync(FULL, myw, (tt + 1u) & 31u);
+                    if (tt + 1u >= tn) w1 = 0u;
+                    if ((w0 | w1) == 0u) continue;
+                    const uint32_t p0 = (uint32_t)__popc(w0);
+                    const uint32_t f0 = (t0 + tt) * 32u + (uint32_t)lane;
+                    if ((w0 >> lane) & 1u) {
+                        uint32_t st = lq[0] + f0;
 #pragma unroll
                         for (int r = 1; r < NR; r++)
-                            if (f >= pq[r]) st = lq[r] + (f - pq[r]);
-                        list[run + (uint32_t)__popc(word & lt)] = a.ids[st];
+                            if (f0 >= pq[r]) st = lq[r] + (f0 - pq[r]);
+                        list[run + (uint32_t)__popc(w0 & lt)] = a.ids[st];
                     }
-                    run += (uint32_t)__popc(word);
+                    if ((w1 >> lane) & 1u) {
+                        const uint32_t f1 = f0 + 32u;
+                        uint32_t st = lq[0] + f1;
+#pragma unroll
+                        for (int r = 1; r < NR; r++)
+                            if (f1 >= pq[r]) st = lq[r] + (f1 - pq[r]);
+                        list[run + p0 + (uint32_t)__popc(w1 & lt)] = a.ids[st];
+                    }
+                    run += p0 + (uint32_t)__popc(w1);
                 }
             }
         }

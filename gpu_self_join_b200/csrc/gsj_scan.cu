@@ -80,28 +80,40 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(unsigned long l
 }
 
 // OutT is uint64_t (list offsets) or uint32_t (slot offsets, digit offsets:
-// the caller guarantees that the total fits).
+// the caller guarantees that the total fits).  Warp w of the block owns the
+// tile's elements [w * 512, (w + 1) * 512), read and written as 16 rows of 32
+// consecutive elements (coalesced); each row is scanned across the lanes and
+// carried into the next.
 template <typename OutT>
 __global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint32_t* __restrict__ in, uint64_t n,
                                                             const unsigned long long* __restrict__ tsum,
                                                             uint64_t ntiles, OutT* __restrict__ out) {
-    // each thread owns kScanItems consecutive elements of the tile
-    const uint64_t base = blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    __shared__ unsigned long long wtot[kScanThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr uint64_t kWarpElems = kScanTile / (kScanThreads / 32);
+    const uint64_t base = blockIdx.x * kScanTile + (uint64_t)warp * kWarpElems + lane;
     uint32_t v[kScanItems];
-    unsigned long long s = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
-        const uint64_t e = base + i;
+        const uint64_t e = base + (uint64_t)i * 32u;
         v[i] = e < n ? in[e] : 0u;
-        s += v[i];
     }
-    unsigned long long tot;
-    unsigned long long run = block_excl_scan(s, &tot) + tsum[blockIdx.x];
+    unsigned long long ex[kScanItems];
+    unsigned long long carry = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
-        const uint64_t e = base + i;
-        if (e < n) out[e] = (OutT)run;
-        run += v[i];
+        const unsigned long long inc = warp_incl_scan(v[i], lane);
+        ex[i] = carry + inc - v[i];
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0) wtot[warp] = carry;
+    __syncthreads();
+    unsigned long long pre = tsum[blockIdx.x];
+    for (int w = 0; w < warp; w++) pre += wtot[w];
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) {
+        const uint64_t e = base + (uint64_t)i * 32u;
+        if (e < n) out[e] = (OutT)(pre + ex[i]);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = (OutT)tsum[ntiles];
 }

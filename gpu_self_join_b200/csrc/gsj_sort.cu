@@ -29,9 +29,9 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;                          // keys per thread
+constexpr int kSortItems = 8;                           // keys per thread
 constexpr int kSortTile = kSortThreads * kSortItems;    // keys per tile
-constexpr int kWarpKeys = kSortTile / kSortWarps;       // keys per warp (16 rounds of 32)
+constexpr int kWarpKeys = kSortTile / kSortWarps;       // keys per warp (8 rounds of 32)
 constexpr int kBins = 256;
 static_assert(kSortThreads == kBins, "one thread per digit in the tile prefix");
 
