@@ -395,23 +395,54 @@ def _requests(args) -> None:
         return JoinConfig(indexed_dims=min(6, r.n), reorder=True, shortcircuit=True, ilp=8, stamp=False,
                           query_reorder=True, plain=args.plain)
 
-    for r, x, eps in prepared[:max(3, args.warmup)]:
-        sj.run(x, eps, cfg_of(r))
+    # Workers: long-lived contexts (own stream and memory pool each), one host
+    # thread per context pulling the next request; the library releases the
+    # interpreter lock inside every call, so the joins of different workers
+    # overlap on the GPU.
+    import queue
+    import threading
+
+    workers = [sj] + [SelfJoin(local_rank) for _ in range(max(1, args.workers) - 1)]
+    for wj in workers:
+        for r, x, eps in prepared[:max(3, args.warmup)]:
+            wj.run(x, eps, cfg_of(r))
     torch.cuda.synchronize()
-    lat, pairs, paths = [], 0, {}
+    lat, stats_all = [0.0] * len(prepared), [None] * len(prepared)
+    todo = queue.Queue()
+    for i in range(len(prepared)):
+        todo.put(i)
+
+    def serve(wj):
+        while True:
+            try:
+                i = todo.get_nowait()
+            except queue.Empty:
+                return
+            r, x, eps = prepared[i]
+            t0 = time.perf_counter()
+            stats_all[i] = wj.run(x, eps, cfg_of(r))
+            lat[i] = (time.perf_counter() - t0) * 1e3
+
     t_all = time.perf_counter()
-    for r, x, eps in prepared:
-        t0 = time.perf_counter()
-        st = sj.run(x, eps, cfg_of(r))
-        lat.append((time.perf_counter() - t0) * 1e3)
-        pairs += int(st["total_pairs"])
-        paths[int(st["join_path"])] = paths.get(int(st["join_path"]), 0) + 1
+    threads = [threading.Thread(target=serve, args=(wj,)) for wj in workers]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
     t_all = time.perf_counter() - t_all
-    sj.close()
+    pairs = sum(int(st["total_pairs"]) for st in stats_all)
+    paths = {}
+    for st in stats_all:
+        paths[int(st["join_path"])] = paths.get(int(st["join_path"]), 0) + 1
+    for wj in workers:
+        wj.close()
     lat_sorted = sorted(lat)
 
     def pct(p):
         return lat_sorted[min(len(lat_sorted) - 1, int(round(p / 100.0 * (len(lat_sorted) - 1))))]
+
+    def mean_of(key):
+        return statistics.mean(float(st[key]) for st in stats_all)
 
     line = {
         "metric": "request stream: result pairs/s (256 joins, 90-D workload phase 2)", "value": pairs / t_all,
@@ -423,6 +454,10 @@ def _requests(args) -> None:
                    "dims": sorted({r.n for r, _, _ in prepared}), "result_pairs": pairs,
                    "join_paths": {str(k): v for k, v in sorted(paths.items())}},
         "latency_ms": {"p50": pct(50), "p90": pct(90), "p99": pct(99), "max": lat_sorted[-1]},
+        "workers": len(workers),
+        "mean_ms": {"host_index": mean_of("ms_index"), "host_join": mean_of("ms_join"),
+                    "dev_index": mean_of("dev_ms_index"), "dev_count": mean_of("dev_ms_count"),
+                    "dev_fill": mean_of("dev_ms_fill"), "launches": mean_of("kernel_launches")},
     }
     print(json.dumps(line), flush=True)
 
@@ -595,6 +630,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=256, help="joins in the c5_requests stream")
+    ap.add_argument("--workers", type=int, default=1,
+                    help="c5_requests: concurrent worker contexts (one stream and host thread each)")
     ap.add_argument("--no-screened-vs-plain", action="store_true",
                     help="skip the 18-D / 90-D screened-versus-plain block of the default line")
     ap.add_argument("--sv-steps", type=int, default=3, help="timed joins per arm of the screened-vs-plain block")

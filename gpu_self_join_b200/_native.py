@@ -32,7 +32,7 @@ EXPORTED_SYMBOLS = (
     "gsj_threshold_f32", "gsj_threshold_f64", "GDSJoinPy", "copyResultIntoPythonArray", "GDSJoinPy_f32",
     "GDSJoinPy_f64", "copyResultIntoPythonArray64", "gsj_list_offsets_noalloc", "gsj_bruteforce_count",
     "gsj_join_host", "gsj_model_train", "gsj_model_reset", "gsj_model_weights", "gsj_model_features",
-    "gsj_model_predict", "gsj_model_loss_grad",
+    "gsj_model_predict", "gsj_model_loss_grad", "gsj_autotune", "gsj_tuning_get", "gsj_tuning_set",
 )
 MODEL_WEIGHTS = 3201
 MODEL_FEATURES = 16
@@ -79,8 +79,22 @@ class GsjStats(ctypes.Structure):
         ("screen_rechecks", ctypes.c_uint64),
         ("reruns", ctypes.c_uint64),
         ("batches", ctypes.c_uint64),
+        ("tuned", ctypes.c_uint64),
+        ("density_log2", ctypes.c_uint64),
         ("estimate", ctypes.c_uint64),
         ("dev_ms_estimate", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class GsjTuning(ctypes.Structure):
+    _fields_ = [
+        ("threads", ctypes.c_uint32),
+        ("warps", ctypes.c_uint32),
+        ("ctas_per_sm", ctypes.c_uint32),
+        ("streams", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -127,6 +141,10 @@ def lib() -> ctypes.CDLL:
     L.gsj_list_offsets_noalloc.argtypes = [P, u64, P, P]
     L.gsj_bruteforce_count.argtypes = [P, P, u64, ctypes.c_double, ctypes.POINTER(GsjConfig), i32, P,
                                        ctypes.POINTER(u64)]
+    L.gsj_autotune.argtypes = [P, P, u64, ctypes.c_double, ctypes.POINTER(GsjConfig), i32, u32,
+                               ctypes.POINTER(GsjTuning)]
+    L.gsj_tuning_get.argtypes = [P, u32, u32, u32, ctypes.POINTER(GsjTuning)]
+    L.gsj_tuning_set.argtypes = [P, u32, u32, u32, ctypes.POINTER(GsjTuning)]
     L.gsj_model_train.argtypes = [P, u32, P]
     L.gsj_model_reset.argtypes = [P]
     L.gsj_model_weights.argtypes = [P, P, u32, i32]

@@ -23,8 +23,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <thread>
 #include <type_traits>
 #include <vector>
@@ -180,6 +182,9 @@ struct gsj_context {
         float log2_eps = 0;
         JoinArgs<float> lookup{};
     } last;
+    // tuned launch shapes by (path, dim, density_log2)
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, gsj_tuning> tuning;
+    const gsj_tuning* forced = nullptr;  // the autotuner's candidate, in place of the table
     // last result
     bool have_result = false;
     uint64_t N = 0, R = 0;
@@ -215,7 +220,7 @@ int dev_get(gsj_context* c, Buf& b, size_t count, X** out) {
         if (b.p) cudaFree(b.p);
         b.p = nullptr;
         b.cap = 0;
-        size_t want = bytes + bytes / 8;  // headroom for slightly larger repeats
+        size_t want = bytes + bytes / 2;  // headroom: a stream of growing joins re-allocates rarely
         cudaError_t e = cudaMalloc(&b.p, want);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -1061,6 +1066,23 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
                  screen_supported(n, npad, k, model, cfg.ilp, threshold_of<float>(eps));
     }
     const uint32_t qchunk = screen ? (uint32_t)kScreenQ : tile ? (uint32_t)kTileQ : (uint32_t)kQChunk;
+    // launch shape: the autotuner's candidate, else the table's entry for this
+    // (path, dim, density), else the launchers' defaults
+    const uint32_t path_id = tpq ? GSJ_PATH_ROWS : screen ? GSJ_PATH_SCREEN : tile ? GSJ_PATH_TILE : GSJ_PATH_WARP;
+    uint32_t dlog = 0;
+    while (dlog < 31 && (N / std::max<uint32_t>(M, 1u)) >> (dlog + 1)) dlog++;
+    S.density_log2 = dlog;
+    gsj_tuning shape{};
+    if (c->forced) {
+        shape = *c->forced;
+        S.tuned = 1;
+    } else {
+        auto it = c->tuning.find(std::make_tuple(path_id, n, dlog));
+        if (it != c->tuning.end()) {
+            shape = it->second;
+            S.tuned = 1;
+        }
+    }
 
     // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525)
     uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
@@ -1138,6 +1160,9 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     for (uint32_t j = 0; j < k; j++) a.minv[j] = minArr[j];
     a.fwd_cnt = fwd;
     a.cand_cnt = cand;
+    a.shape_threads = shape.threads;
+    a.shape_warps = shape.warps;
+    a.shape_per_sm = shape.ctas_per_sm;
     const bool stamp = cfg.stamp != 0 && !(cfg.flags & GSJ_FLAG_NO_UNICOMP);
     const bool exact_size = (cfg.flags & GSJ_FLAG_EXACT_SIZE) != 0;
     // the cell table of this join, for the model's features (estimate now,
@@ -1205,7 +1230,9 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
             c->R = R;
             return GSJ_ERR_OVERFLOW;
         }
-        GSJ_TRY(rows_to_host<T>(c, a, cfg, N, R, slot_cell, bitoff, hitbits, counts, offsets, *ho));
+        gsj_config pcfg = cfg;
+        if (shape.streams) pcfg.streams = shape.streams;
+        GSJ_TRY(rows_to_host<T>(c, a, pcfg, N, R, slot_cell, bitoff, hitbits, counts, offsets, *ho));
         {
             float ms = 0;
             GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
@@ -1417,6 +1444,84 @@ int gsj_join_host(gsj_context* c, const void* data, uint64_t num_points, double 
     c->stats.ms_total = now_ms() - t0;
     if (stats) *stats = c->stats;
     return r;
+}
+
+static int tuning_valid(gsj_context* c, const gsj_tuning& t) {
+    if (t.threads && (t.threads < 64 || t.threads > 256 || (t.threads & 31u)))
+        return fail(c, GSJ_ERR_INVALID, "tuning: threads must be 64..256, a multiple of 32");
+    if (t.warps > 8) return fail(c, GSJ_ERR_INVALID, "tuning: warps must be at most 8");
+    if (t.streams > (uint32_t)gsj_context::kMaxSeg) return fail(c, GSJ_ERR_INVALID, "tuning: at most 8 streams");
+    return GSJ_OK;
+}
+
+int gsj_tuning_get(gsj_context* c, uint32_t path, uint32_t dim, uint32_t dlog, gsj_tuning* t) {
+    if (!c || !t) return fail(c, GSJ_ERR_INVALID, "null argument");
+    auto it = c->tuning.find(std::make_tuple(path, dim, dlog));
+    if (it == c->tuning.end()) return fail(c, GSJ_ERR_STATE, "no tuning entry for this key");
+    *t = it->second;
+    return GSJ_OK;
+}
+
+int gsj_tuning_set(gsj_context* c, uint32_t path, uint32_t dim, uint32_t dlog, const gsj_tuning* t) {
+    if (!c || !t) return fail(c, GSJ_ERR_INVALID, "null argument");
+    GSJ_TRY(tuning_valid(c, *t));
+    c->tuning[std::make_tuple(path, dim, dlog)] = *t;
+    return GSJ_OK;
+}
+
+int gsj_autotune(gsj_context* c, const void* data, uint64_t num_points, double eps, const gsj_config* cfg,
+                 int data_on_device, uint32_t repeats, gsj_tuning* best) {
+    if (!c || !cfg || !best) return fail(c, GSJ_ERR_INVALID, "null argument");
+    if (repeats == 0) repeats = 1;
+    gsj_stats st{};
+    // the path and density of this join, under the current shape
+    GSJ_TRY(gsj_join(c, data, num_points, eps, cfg, data_on_device, &st));
+    if (num_points == 0) return fail(c, GSJ_ERR_INVALID, "nothing to tune on an empty input");
+    const uint32_t path = (uint32_t)st.join_path, dlog = (uint32_t)st.density_log2;
+    gsj_tuning cur{};
+    {
+        auto it = c->tuning.find(std::make_tuple(path, cfg->dim, dlog));
+        if (it != c->tuning.end()) cur = it->second;
+    }
+    auto timed = [&](const gsj_tuning& t, double* ms) -> int {
+        c->forced = &t;
+        int r = gsj_join(c, data, num_points, eps, cfg, data_on_device, &st);  // warm-up
+        double sum = 0.0;
+        for (uint32_t i = 0; r == GSJ_OK && i < repeats; i++) {
+            r = gsj_join(c, data, num_points, eps, cfg, data_on_device, &st);
+            sum += st.dev_ms_index + st.dev_ms_count + st.dev_ms_fill;
+        }
+        c->forced = nullptr;
+        *ms = sum / repeats;
+        return r;
+    };
+    // the knobs of the path and their candidate values (0 = the default)
+    std::vector<std::pair<uint32_t gsj_tuning::*, std::vector<uint32_t>>> knobs;
+    if (path == GSJ_PATH_ROWS) knobs.push_back({&gsj_tuning::threads, {0, 128, 192}});
+    if (path == GSJ_PATH_WARP) {
+        knobs.push_back({&gsj_tuning::warps, {0, 4, 2}});
+        knobs.push_back({&gsj_tuning::ctas_per_sm, {0, 4, 2}});
+    }
+    if (path == GSJ_PATH_TILE) knobs.push_back({&gsj_tuning::ctas_per_sm, {0, 2, 1}});
+    if (path == GSJ_PATH_SCREEN) knobs.push_back({&gsj_tuning::ctas_per_sm, {0, 1}});
+    double best_ms = 0.0;
+    GSJ_TRY(timed(cur, &best_ms));
+    for (auto& kv : knobs) {
+        for (uint32_t v : kv.second) {
+            gsj_tuning cand = cur;
+            cand.*(kv.first) = v;
+            if (cand.*(kv.first) == cur.*(kv.first)) continue;
+            double ms = 0.0;
+            GSJ_TRY(timed(cand, &ms));
+            if (ms < best_ms) {
+                best_ms = ms;
+                cur = cand;
+            }
+        }
+    }
+    c->tuning[std::make_tuple(path, cfg->dim, dlog)] = cur;
+    *best = cur;
+    return GSJ_OK;
 }
 
 int gsj_bruteforce_count(gsj_context* c, const void* data, uint64_t num_points, double eps, const gsj_config* cfg,

@@ -56,6 +56,10 @@ struct JoinArgs {
     uint32_t* table;              // [R]
     unsigned long long table_cap; // R: writes at or beyond it are dropped and flagged
     uint32_t* err_flag;           // set to 1 when a write would leave the table
+    // launch shape of this join (0 = the launcher's default), from the tuning table
+    uint32_t shape_threads;       // ROWS count / fill CTA size (64..256, a multiple of 32)
+    uint32_t shape_warps;         // WARP join: warps per CTA (1..8)
+    uint32_t shape_per_sm;        // WARP, TILE, SCREEN joins: CTAs per SM at most
 };
 
 __host__ __device__ inline uint64_t mix64(uint64_t x) {

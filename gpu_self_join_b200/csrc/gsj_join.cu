@@ -341,6 +341,7 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     const uint32_t max_smem = 200u * 1024u;
     int warps = (int)(max_smem / L.total);
     if (warps > 8) warps = 8;
+    if (a.shape_warps && (int)a.shape_warps < warps) warps = (int)a.shape_warps;
     if (warps < 1) return cudaErrorInvalidValue;
     const int threads = warps * 32;
     const size_t smem = (size_t)warps * L.total;
@@ -354,6 +355,7 @@ static cudaError_t launch_one(const JoinArgs<T>& a, uint32_t nb_cap, uint32_t no
     e = blocks_per_sm((const void*)kern, threads, smem, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
+    if (a.shape_per_sm && (int)a.shape_per_sm < per_sm) per_sm = (int)a.shape_per_sm;
     const uint64_t needed = ((uint64_t)nvisit + warps - 1) / warps;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > needed) blocks = needed ? needed : 1;

@@ -633,6 +633,7 @@ cudaError_t launch_screen_one(const JoinArgs<float>& a, const TileOut& o, const 
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     // tensor memory: 2 accumulators of 128 columns per CTA, 512 columns per SM
     if ((uint32_t)per_sm * 2u * kTmemCols > 512u) per_sm = (int)(512u / (2u * kTmemCols));
+    if (a.shape_per_sm && (int)a.shape_per_sm < per_sm) per_sm = (int)a.shape_per_sm;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > nvisit) blocks = nvisit ? nvisit : 1;
     kern<<<(unsigned)blocks, kSThreads, smem, st>>>(a, o, sc, noff, nvisit);

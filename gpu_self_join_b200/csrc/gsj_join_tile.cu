@@ -351,6 +351,7 @@ cudaError_t launch_tile_one(const JoinArgs<float>& a, const TileOut& o, uint32_t
     e = blocks_per_sm((const void*)kern, kThreads, L.total, &per_sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if (a.shape_per_sm && (int)a.shape_per_sm < per_sm) per_sm = (int)a.shape_per_sm;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > nvisit) blocks = nvisit ? nvisit : 1;
     kern<<<(unsigned)blocks, kThreads, L.total, st>>>(a, o, noff, nvisit);

@@ -243,10 +243,11 @@ static cudaError_t launch_count_nt(const JoinArgs<T>& a, const uint32_t* slot_ce
                                    uint32_t* bits, uint32_t* counts_by_id, int num_sms, cudaStream_t st) {
     constexpr int POL = sizeof(T) == 8 ? kPolF64 : kPolF32;
     auto kern = k_rows_count<T, NT, NR, POL>;
-    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, 256, 0, num_sms);
-    const uint64_t needed = ((uint64_t)a.n_points + 255) / 256;
+    const int threads = a.shape_threads ? (int)a.shape_threads : 256;
+    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, threads, 0, num_sms);
+    const uint64_t needed = ((uint64_t)a.n_points + threads - 1) / threads;
     if (blocks > needed) blocks = needed ? needed : 1;
-    kern<<<(unsigned)blocks, 256, 0, st>>>(a, slot_cell, bitoff, bits, counts_by_id);
+    kern<<<(unsigned)blocks, threads, 0, st>>>(a, slot_cell, bitoff, bits, counts_by_id);
     return cudaGetLastError();
 }
 
@@ -282,10 +283,11 @@ static cudaError_t fill_nr(const JoinArgs<float>& a, const uint32_t* slot_cell, 
                            cudaStream_t st) {
     if (nq == 0) return cudaSuccess;
     auto kern = k_rows_fill<NR>;
-    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, 256, 0, num_sms);
-    const uint64_t needed = ((uint64_t)nq + 255) / 256;
+    const int threads = a.shape_threads ? (int)a.shape_threads : 256;
+    uint64_t blocks = (uint64_t)resident_blocks((const void*)kern, threads, 0, num_sms);
+    const uint64_t needed = ((uint64_t)nq + threads - 1) / threads;
     if (blocks > needed) blocks = needed ? needed : 1;
-    kern<<<(unsigned)blocks, 256, 0, st>>>(a, slot_cell, bitoff, bits, qslots, nq, base);
+    kern<<<(unsigned)blocks, threads, 0, st>>>(a, slot_cell, bitoff, bits, qslots, nq, base);
     return cudaGetLastError();
 }
 
@@ -307,6 +309,7 @@ cudaError_t launch_rows_fill(const JoinArgs<T>& a, const uint32_t* slot_cell, co
     f.table = a.table;
     f.table_cap = a.table_cap;
     f.err_flag = a.err_flag;
+    f.shape_threads = a.shape_threads;
     if (a.g.k == 1) return fill_nr<1>(f, slot_cell, bitoff, bits, qslots, nq, base, num_sms, st);
     if (a.g.k == 2) return fill_nr<3>(f, slot_cell, bitoff, bits, qslots, nq, base, num_sms, st);
     return fill_nr<9>(f, slot_cell, bitoff, bits, qslots, nq, base, num_sms, st);

@@ -11,31 +11,9 @@ namespace gsj {
 // Resident CTAs per SM for a launch: the larger of the occupancy calculation
 // and the same fit computed from the SM's limits (shared memory with the
 // per-block reservation, registers in 256-register warp units, threads),
-// since the calculation can come out below what the SM holds.
-inline cudaError_t blocks_per_sm(const void* kern, int threads, size_t smem, int* per_sm) {
-    int api = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&api, kern, threads, smem);
-    if (e != cudaSuccess) return e;
-    cudaFuncAttributes fa{};
-    int dev = 0, smem_sm = 0, resv = 0, regs_sm = 0, thr_sm = 0;
-    if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) == cudaSuccess) {
-        const long long blk_smem = (long long)smem + resv + (long long)fa.sharedSizeBytes;
-        const long long warp_regs = ((long long)fa.numRegs * 32 + 255) / 256 * 256;
-        const long long blk_regs = warp_regs * ((threads + 31) / 32);
-        long long fit = (long long)thr_sm / threads;
-        if (blk_smem > 0 && smem_sm / blk_smem < fit) fit = smem_sm / blk_smem;
-        if (blk_regs > 0 && regs_sm / blk_regs < fit) fit = regs_sm / blk_regs;
-        if (fit > api) api = (int)fit;
-    } else {
-        cudaGetLastError();
-    }
-    *per_sm = api;
-    return cudaSuccess;
-}
+// since the calculation can come out below what the SM holds.  Results are
+// cached per (device, kernel, block size, dynamic shared memory).
+cudaError_t blocks_per_sm(const void* kern, int threads, size_t smem, int* per_sm);
 
 constexpr unsigned kVarStageBytes = 98304;  // shared staging of sampled rows (REORDER statistic)
 

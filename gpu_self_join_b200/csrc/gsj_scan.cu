@@ -10,10 +10,12 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <map>
 #include <mutex>
 #include <string>
 
 #include "../../include/gpuselfjoin.h"
+#include "gsj_kernels.h"
 #include "gsj_scan.h"
 
 namespace gsj {
@@ -137,6 +139,63 @@ cudaError_t scan_u32_u64(const uint32_t* in, uint64_t* out, uint64_t n, void* te
 
 cudaError_t scan_u32_u32(const uint32_t* in, uint32_t* out, uint64_t n, void* temp, cudaStream_t st) {
     return scan_any<uint32_t>(in, out, n, temp, st);
+}
+
+// ---------------------------------------------------------------- launch shapes
+namespace {
+struct OccKey {
+    int dev;
+    const void* kern;
+    int threads;
+    size_t smem;
+    bool operator<(const OccKey& o) const {
+        if (dev != o.dev) return dev < o.dev;
+        if (kern != o.kern) return kern < o.kern;
+        if (threads != o.threads) return threads < o.threads;
+        return smem < o.smem;
+    }
+};
+std::mutex g_occ_mu;
+std::map<OccKey, int> g_occ;
+}  // namespace
+
+cudaError_t blocks_per_sm(const void* kern, int threads, size_t smem, int* per_sm) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const OccKey key{dev, kern, threads, smem};
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        auto it = g_occ.find(key);
+        if (it != g_occ.end()) {
+            *per_sm = it->second;
+            return cudaSuccess;
+        }
+    }
+    int api = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&api, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa{};
+    int smem_sm = 0, resv = 0, regs_sm = 0, thr_sm = 0;
+    if (cudaFuncGetAttributes(&fa, kern) == cudaSuccess &&
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) == cudaSuccess) {
+        const long long blk_smem = (long long)smem + resv + (long long)fa.sharedSizeBytes;
+        const long long warp_regs = ((long long)fa.numRegs * 32 + 255) / 256 * 256;
+        const long long blk_regs = warp_regs * ((threads + 31) / 32);
+        long long fit = (long long)thr_sm / threads;
+        if (blk_smem > 0 && smem_sm / blk_smem < fit) fit = smem_sm / blk_smem;
+        if (blk_regs > 0 && regs_sm / blk_regs < fit) fit = regs_sm / blk_regs;
+        if (fit > api) api = (int)fit;
+    } else {
+        cudaGetLastError();
+    }
+    *per_sm = api;
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    g_occ[key] = api;
+    return cudaSuccess;
 }
 
 // ---------------------------------------------------------------- no allocation

@@ -155,6 +155,43 @@ class SelfJoin:
         self.N, self.n = Np, n
         return st.as_dict(), counts, table[: int(total.value)]
 
+    # ---- launch-shape tuning
+    def _points_arg(self, points):
+        if hasattr(points, "is_cuda") and points.is_cuda:
+            import torch
+
+            dt = np.float64 if points.dtype == torch.float64 else np.float32
+            return ctypes.c_void_p(points.data_ptr()), points.shape, dt, 1, points
+        p = np.ascontiguousarray(points)
+        if p.dtype not in (np.float32, np.float64):
+            p = p.astype(np.float32)
+        return ctypes.c_void_p(p.ctypes.data), p.shape, p.dtype, 0, p
+
+    def autotune(self, points, eps: float, config: JoinConfig | None = None, repeats: int = 2, **kw) -> dict:
+        """Times the join of `points` under candidate launch shapes of the path
+        it takes and keeps the fastest in this context's tuning table;
+        returns the chosen shape."""
+        cfg = config or JoinConfig(**kw)
+        ptr, shape, dt, on_dev, keep = self._points_arg(points)
+        c = self._cfg(shape[1], dt, cfg)
+        t = N.GsjTuning()
+        N.check(self._L.gsj_autotune(self._ctx, ptr, shape[0], float(eps), ctypes.byref(c), on_dev, int(repeats),
+                                     ctypes.byref(t)), self._ctx)
+        del keep
+        return t.as_dict()
+
+    def tuning(self, path: int, dim: int, density_log2: int, shape: dict | None = None) -> dict | None:
+        """The tuning-table entry of (path, dim, density_log2); with `shape`,
+        sets it first.  None when there is no entry."""
+        t = N.GsjTuning()
+        if shape is not None:
+            for k, v in shape.items():
+                setattr(t, k, int(v))
+            N.check(self._L.gsj_tuning_set(self._ctx, path, dim, density_log2, ctypes.byref(t)), self._ctx)
+        if self._L.gsj_tuning_get(self._ctx, path, dim, density_log2, ctypes.byref(t)) != N.GSJ_OK:
+            return None
+        return t.as_dict()
+
     # ---- learned result-count model (GSJ_EST_LEARNED)
     def model_train(self, steps: int = 400) -> float:
         """Trains the context's model on the exact counts of the last join;

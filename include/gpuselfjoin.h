@@ -122,6 +122,9 @@ typedef struct gsj_stats {
     uint64_t reruns;          /* passes repeated because a buffer sized from the
                                  estimate was short (the output is unchanged)  */
     uint64_t batches;         /* result batches of gsj_join_host (1 otherwise)  */
+    uint64_t tuned;           /* 1 when a tuning-table entry shaped the launches */
+    uint64_t density_log2;    /* floor(log2(points per non-empty cell)): the
+                                 tuning table's density key                    */
     uint64_t estimate;        /* pairs (or undecided pairs) the estimator
                                  predicted for the exact pass                  */
     double dev_ms_estimate;   /* device time of the estimate                    */
@@ -243,6 +246,34 @@ GSJ_API int gsj_bruteforce_count(gsj_context* ctx, const void* data, uint64_t nu
  * the caller.
  */
 GSJ_API int gsj_list_offsets_noalloc(const uint32_t* d_counts, uint64_t n, uint64_t* d_offsets, void* stream);
+
+/* ---------------------------------------------------------------- autotuning
+ * Launch shapes chosen per (join path, dimensionality, density).  The
+ * reference fixes them at compile time (BLOCKSIZE, params.h:17; GPUSTREAMS,
+ * params.h:85).  A context keeps a table of tuned shapes; a join whose
+ * (path, dim, density_log2) has an entry launches with it (gsj_stats.tuned).
+ * Shapes never change results, only speed. */
+typedef struct gsj_tuning {
+    uint32_t threads;     /* ROWS path: CTA size of the count and fill passes
+                             (64..256, a multiple of 32; 0: 256)              */
+    uint32_t warps;       /* WARP path: warps per CTA (1..8; 0: as many as the
+                             shared memory allows, up to 8)                   */
+    uint32_t ctas_per_sm; /* WARP, TILE, SCREEN paths: resident CTAs per SM at
+                             most (0: all that fit)                           */
+    uint32_t streams;     /* gsj_join_host: segments in flight (0: the config's) */
+} gsj_tuning;
+
+/* Times the join of `data` under candidate shapes of the path it takes
+ * (coordinate descent, each candidate the mean device time of `repeats`
+ * joins after one warm-up), stores the fastest in the context's table for the
+ * join's (path, dim, density_log2) and returns it in *best. */
+GSJ_API int gsj_autotune(gsj_context* ctx, const void* data, uint64_t num_points, double eps, const gsj_config* cfg,
+                         int data_on_device, uint32_t repeats, gsj_tuning* best);
+/* Reads (GSJ_ERR_STATE when absent) or writes one table entry, e.g. to keep
+ * tuned shapes across processes. */
+GSJ_API int gsj_tuning_get(gsj_context* ctx, uint32_t path, uint32_t dim, uint32_t density_log2, gsj_tuning* t);
+GSJ_API int gsj_tuning_set(gsj_context* ctx, uint32_t path, uint32_t dim, uint32_t density_log2,
+                           const gsj_tuning* t);
 
 /* ---------------------------------------------------------------- learned
  * The context's result-count model (GSJ_EST_LEARNED): a 16-64-32-1 MLP
