@@ -54,7 +54,7 @@ class GsjConfig(ctypes.Structure):
         ("streams", ctypes.c_uint32),
         ("min_batches", ctypes.c_uint32),
         ("estimator", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("sort", ctypes.c_uint32),
     ]
 
 

@@ -28,7 +28,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgpuselfjoin.so")
 CLI = os.path.join(HERE, "main")
 
-CU_SOURCES = ["gsj_index.cu", "gsj_join.cu", "gsj_join_tpq.cu", "gsj_join_tile.cu", "gsj_join_screen.cu", "gsj_bruteforce.cu", "gsj_scan.cu", "gsj_sort.cu", "gsj_place.cu", "gsj_model.cu", "gsj_api.cu"]
+CU_SOURCES = ["gsj_index.cu", "gsj_join.cu", "gsj_join_tpq.cu", "gsj_join_tile.cu", "gsj_join_screen.cu", "gsj_join_sort.cu", "gsj_bruteforce.cu", "gsj_scan.cu", "gsj_sort.cu", "gsj_place.cu", "gsj_model.cu", "gsj_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "--expt-relaxed-constexpr", "-Xptxas", "-v", "-ccbin", "g++"]

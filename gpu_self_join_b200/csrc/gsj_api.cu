@@ -68,6 +68,9 @@
 #ifndef QUERYREORDER
 #define QUERYREORDER 0
 #endif
+#ifndef SORT
+#define SORT 0
+#endif
 
 using namespace gsj;
 
@@ -126,6 +129,18 @@ double threshold_of<double>(double eps) {
     return s;
 }
 
+// SORT's per-cell element and order (GPU.cu:51-54): kept as the reference
+// declares them so that std::sort orders ties the same way.
+template <typename T>
+struct key_val_sort {
+    unsigned int pid;
+    T value_at_dim;
+};
+template <typename T>
+bool compareByPointValue(const key_val_sort<T>& a, const key_val_sort<T>& b) {
+    return a.value_at_dim < b.value_at_dim;
+}
+
 template <typename T>
 struct dim_reorder_sort {  // structs.h:37-41
     unsigned int dim;
@@ -160,7 +175,7 @@ struct gsj_context {
     Buf in, pts, ids, keys, keys2, vals, cell_key, cell_start, dense, dcnt, plan, plan_par, slot_cell, hkeys, hvals, order,
         sizes, nchunks,
         item_off, items, fwd, swords, counts, offsets, table, temp, scan_temp, misc, var, perm, minarr,
-        minmax_part, pairs, srows, snorms, spartial, scentre, unc, table2, nbtab, bitoff, hitbits, ptemp;
+        minmax_part, pairs, srows, snorms, spartial, scentre, unc, table2, nbtab, bitoff, hitbits, ptemp, sortv;
     PinnedBuf stage[2];
     PinnedBuf hmisc;
     // host-result pipeline: copy streams, per-segment events, pinned staging
@@ -806,6 +821,63 @@ int rows_to_host(gsj_context* c, JoinArgs<T>& a, const gsj_config& cfg, uint64_t
     return GSJ_OK;
 }
 
+// ------------------------------------------------------------------ SORT path
+// The reference's SORT traversal (kernel.cu:400-467), thread per query: count
+// pass, list offsets, fill pass writing every list in candidate order.
+template <typename T>
+int sort_join(gsj_context* c, JoinArgs<T>& a, uint64_t N, int model, uint32_t* counts, uint64_t* offsets,
+              const uint32_t* cell_start, uint32_t M, double t_join, double t_start) {
+    gsj_stats& S = c->stats;
+    cudaStream_t st = c->st;
+    uint32_t* slot_cell = nullptr;
+    GSJ_TRY(dev_get(c, c->slot_cell, N, &slot_cell));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_slot_cell(cell_start, M, nullptr, 0, slot_cell, nullptr, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[2], st));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_sort_join<T>(a, slot_cell, counts, model, false, c->num_sms, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[3], st));
+    void* stemp = nullptr;
+    GSJ_TRY(dev_get(c, c->scan_temp, scan_u32_u64_temp_bytes(N), (unsigned char**)&stemp));
+    S.kernel_launches += 3;
+    GSJ_CUDA(c, scan_u32_u64(counts, offsets, N, stemp, st));
+    uint64_t R = 0;
+    GSJ_TRY(d2h_small(c, &R, offsets + N, 1));
+    uint32_t* table = nullptr;
+    GSJ_TRY(dev_get(c, c->table, R ? R : 1, &table));
+    a.offsets = offsets;
+    a.table = table;
+    a.table_cap = R;
+    a.err_flag = a.work_counter + 1;
+    GSJ_CUDA(c, cudaEventRecord(c->tev[4], st));
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_sort_join<T>(a, slot_cell, counts, model, true, c->num_sms, st));
+    GSJ_CUDA(c, cudaEventRecord(c->tev[5], st));
+    GSJ_CUDA(c, cudaStreamSynchronize(st));
+    uint32_t err = 0;
+    GSJ_TRY(d2h_small(c, &err, a.err_flag, 1));
+    if (err) return fail(c, GSJ_ERR_STATE, "SORT fill pass disagreed with its count pass (internal error)");
+    unsigned long long ncand = 0;
+    GSJ_TRY(d2h_small(c, &ncand, a.cand_cnt, 1));
+    {
+        float ms = 0;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
+        S.dev_ms_index = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[2], c->tev[3]));
+        S.dev_ms_count = ms;
+        GSJ_CUDA(c, cudaEventElapsedTime(&ms, c->tev[4], c->tev[5]));
+        S.dev_ms_fill = ms;
+    }
+    S.candidates = ncand;
+    S.total_pairs = R;
+    S.join_path = GSJ_PATH_SORT;
+    c->R = R;
+    c->have_result = true;
+    S.ms_join = now_ms() - t_join;
+    S.ms_total = now_ms() - t_start;
+    return GSJ_OK;
+}
+
 // ------------------------------------------------------------------ join
 template <typename T>
 int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const gsj_config& cfg, int on_dev,
@@ -989,6 +1061,38 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     GSJ_TRY(d2h_small(c, &M, d_nruns, 1));
     S.nonempty_cells = M;
 
+    // ---- SORT (GPU.cu:351-395): each cell's points ordered by their value in the
+    // sort dimension with std::sort and the reference's comparator, on the host
+    // as the reference does (the tie order is std::sort's)
+    if (cfg.sort && N > 1) {
+        const uint32_t sd = n > k ? k : 0u;
+        T* d_sv = reinterpret_cast<T*>(vals);  // the sort's value buffer is free now
+        if (sizeof(T) > sizeof(uint32_t)) GSJ_TRY(dev_get(c, c->sortv, N, &d_sv));
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_sort_values<T>(d_in, N, n, perm[sd], ids, d_sv, st));
+        std::vector<T> hv(N);
+        std::vector<uint32_t> hid(N), hcs(M + 1);
+        GSJ_CUDA(c, cudaMemcpyAsync(hv.data(), d_sv, N * sizeof(T), cudaMemcpyDeviceToHost, st));
+        GSJ_CUDA(c, cudaMemcpyAsync(hid.data(), ids, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        GSJ_CUDA(c, cudaMemcpyAsync(hcs.data(), cell_start, (M + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        GSJ_CUDA(c, cudaStreamSynchronize(st));
+        const unsigned nt = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 16u);
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; t++)
+            th.emplace_back([&, t] {
+                std::vector<key_val_sort<T>> tmp;
+                for (uint64_t cc = t; cc < M; cc += nt) {
+                    tmp.clear();
+                    for (uint32_t s2 = hcs[cc]; s2 < hcs[cc + 1]; s2++) tmp.push_back({hid[s2], hv[s2]});
+                    std::sort(tmp.begin(), tmp.end(), compareByPointValue<T>);
+                    for (size_t x = 0; x < tmp.size(); x++) hid[hcs[cc] + x] = tmp[x].pid;
+                }
+            });
+        for (auto& x : th) x.join();
+        GSJ_CUDA(c, cudaMemcpyAsync(ids, hid.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        GSJ_CUDA(c, cudaStreamSynchronize(st));
+    }
+
     // ---- points in cell order
     T* pts = nullptr;
     GSJ_TRY(dev_get(c, c->pts, N * npad, &pts));
@@ -1038,7 +1142,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     }
     uint32_t* slot_cell = nullptr;
     uint64_t* bitoff = nullptr;
-    const bool tpq = rows && cfg.ilp == 0 && n <= 4;
+    const bool tpq = rows && cfg.ilp == 0 && n <= 4 && !cfg.sort;
     if (tpq) {
         // slot -> cell, and the hit-mask layout: slot s's query owns words
         // [bitoff[s], bitoff[s+1]) of the count pass's bit masks
@@ -1061,14 +1165,18 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     const int model = model_of(cfg);
     bool tile = false, screen = false;
     if constexpr (std::is_same<T, float>::value) {
-        tile = tile_supported(n, npad, k, model, cfg.ilp) && N >= 8ull * M;
+        tile = !cfg.sort && tile_supported(n, npad, k, model, cfg.ilp) && N >= 8ull * M;
         screen = tile && !(cfg.flags & GSJ_FLAG_PLAIN) &&
                  screen_supported(n, npad, k, model, cfg.ilp, threshold_of<float>(eps));
     }
     const uint32_t qchunk = screen ? (uint32_t)kScreenQ : tile ? (uint32_t)kTileQ : (uint32_t)kQChunk;
     // launch shape: the autotuner's candidate, else the table's entry for this
     // (path, dim, density), else the launchers' defaults
-    const uint32_t path_id = tpq ? GSJ_PATH_ROWS : screen ? GSJ_PATH_SCREEN : tile ? GSJ_PATH_TILE : GSJ_PATH_WARP;
+    const uint32_t path_id = cfg.sort ? GSJ_PATH_SORT
+                             : tpq    ? GSJ_PATH_ROWS
+                             : screen ? GSJ_PATH_SCREEN
+                             : tile   ? GSJ_PATH_TILE
+                                      : GSJ_PATH_WARP;
     uint32_t dlog = 0;
     while (dlog < 31 && (N / std::max<uint32_t>(M, 1u)) >> (dlog + 1)) dlog++;
     S.density_log2 = dlog;
@@ -1182,6 +1290,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     c->last.lookup.n_points = (uint32_t)N;
     c->last.lookup.ids = ids;
     const bool learned = !exact_size && cfg.estimator == GSJ_EST_LEARNED && c->model_trained;
+    if (cfg.sort) return sort_join<T>(c, a, N, model, counts, offsets, cell_start, M, t_join, t_start);
     if constexpr (std::is_same<T, float>::value) {
         if (tile) {
             unsigned long long* cursor = reinterpret_cast<unsigned long long*>(ctr + 4);
@@ -1327,6 +1436,7 @@ void gsj_default_config(gsj_config* cfg) {
     cfg->ilp = ILP;
     cfg->stamp = (STAMP || LINEARSTAMP) ? 1 : 0;
     cfg->query_reorder = QUERYREORDER;
+    cfg->sort = SORT;
     cfg->device = 0;
     cfg->flags = GSJ_FLAG_QUIET;
 }
@@ -1374,7 +1484,7 @@ int gsj_destroy(gsj_context* c) {
                    &c->nchunks,  &c->item_off, &c->items, &c->fwd,     &c->swords,     &c->counts,    &c->offsets,
                    &c->table, &c->temp,   &c->scan_temp, &c->misc,    &c->var,       &c->perm,
                    &c->minarr,   &c->minmax_part, &c->pairs, &c->srows, &c->snorms,
-                   &c->spartial, &c->scentre, &c->unc, &c->table2, &c->nbtab, &c->bitoff, &c->hitbits, &c->ptemp};
+                   &c->spartial, &c->scentre, &c->unc, &c->table2, &c->nbtab, &c->bitoff, &c->hitbits, &c->ptemp, &c->sortv};
     for (Buf* b : bufs)
         if (b->p) cudaFree(b->p);
     for (auto* pb : {&c->stage[0], &c->stage[1], &c->hmisc})

@@ -119,3 +119,40 @@ __device__ __forceinline__ T sqdist_generic(const T* __restrict__ q, const T* __
 }
 
 }  // namespace gsj
+
+namespace gsj {
+
+// The same models for one thread on its own (no warp-wide early exit, so it
+// may run in divergent code): q and c are rows of n values in global memory.
+// Leaving out the early exit never changes a decision.
+template <typename T, int MODEL, int POL>
+__device__ __forceinline__ T sqdist_lane(const T* __restrict__ q, const T* __restrict__ c, uint32_t n,
+                                         uint32_t ilp) {
+    if (MODEL == kSeq) {
+        Acc<T, POL> s;
+        for (uint32_t l = 0; l < n; l++) s.add_prod(FP<T>::sub(c[l], q[l]));
+        return s.v;
+    } else if (MODEL == kIlp) {
+        Acc<T, POL> s;
+        for (uint32_t j = 0; j < ilp; j++) {
+            Acc<T, POL> r;
+            for (uint32_t l = j; l < n; l += ilp) r.add_prod(FP<T>::sub(c[l], q[l]));
+            if (j == 0) s = r;
+            else s.add_acc(r);
+        }
+        return s.v;
+    } else {
+        Acc<T, POL> r0;
+        for (uint32_t l = 0; l < n; l += ilp) {
+            r0.add_prod(FP<T>::sub(c[l], q[l]));
+            for (uint32_t j = 1; j < ilp && l + j < n; j++) {
+                Acc<T, POL> rj;
+                rj.add_prod(FP<T>::sub(c[l + j], q[l + j]));
+                r0.add_acc(rj);
+            }
+        }
+        return r0.v;
+    }
+}
+
+}  // namespace gsj

@@ -86,6 +86,18 @@ cudaError_t launch_group_starts(const uint32_t* sorted_bkey, uint32_t N, uint32_
 // *out = max of in[0 .. n) (*out zeroed by the caller).
 cudaError_t launch_max_u32(const uint32_t* in, uint64_t n, uint32_t* out, cudaStream_t st);
 
+// SORT variant (gsj_join_sort.cu): a count pass (fill == false: list lengths
+// into counts_by_id, candidates into a.cand_cnt) and a fill pass (a.offsets,
+// a.table, a.err_flag set) of the reference's pruned per-cell scans; the
+// points of each cell must be in sort-dimension order.  `model` is one of Model.
+template <typename T>
+cudaError_t launch_sort_join(const JoinArgs<T>& a, const uint32_t* slot_cell, uint32_t* counts_by_id, int model,
+                             bool fill, int num_sms, cudaStream_t st);
+// out[s] = in[ids[s] * n + col]: the sort dimension's values in slot order.
+template <typename T>
+cudaError_t launch_sort_values(const T* in, uint64_t N, uint32_t n, uint32_t col, const uint32_t* ids, T* out,
+                               cudaStream_t st);
+
 // Tile join of high-dimensional float data (5 <= n <= kTileMaxN, k <= 6):
 // a CTA per item of up to kTileQ query slots; hits become packed
 // (query id << shift | candidate id) keys in a pair buffer.

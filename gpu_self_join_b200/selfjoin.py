@@ -38,6 +38,7 @@ class JoinConfig:
     streams: int = 0          # GPUSTREAMS: result segments in flight in run_host (0: 3)
     min_batches: int = 0      # MINBATCHES: fewest result batches of run_host (0: 3)
     learned: bool = False     # size pair buffers with the context's learned result-count model
+    sort: bool = False        # SORT: cells sorted by one dimension, neighbour scans pruned (the reference's pairs)
 
 
 class SelfJoin:
@@ -84,6 +85,7 @@ class SelfJoin:
         c.streams = int(cfg.streams)
         c.min_batches = int(cfg.min_batches)
         c.estimator = N.GSJ_EST_LEARNED if cfg.learned else N.GSJ_EST_SAMPLED
+        c.sort = int(cfg.sort)
         return c
 
     def run(self, points, eps: float, config: JoinConfig | None = None, **kw) -> dict:

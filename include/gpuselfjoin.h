@@ -85,7 +85,10 @@ typedef struct gsj_config {
     uint32_t min_batches;   /* MINBATCHES     fewest batches (0: 3)              */
     uint32_t estimator;     /* GSJ_EST_*      result-size estimate of the pair
                                               paths (SAMPLERATE's role)         */
-    uint32_t reserved;      /* zero                                             */
+    uint32_t sort;          /* SORT           points of each cell ordered by one
+                                              dimension, neighbour scans pruned
+                                              by it (params.h:46); the reference's
+                                              pairs (GSJ_PATH_SORT)               */
 } gsj_config;
 
 /* Result-size estimators (gsj_config.estimator): how the warp, tile and screen
@@ -138,6 +141,8 @@ typedef struct gsj_stats {
 #define GSJ_PATH_SCREEN 3u /* float, 16 <= n <= 128, k <= 6, >= 8 points per cell:
                              BF16 tcgen05 screen with a proven bound, exact FP32
                              check of the rest, pair buffer, on-device sort   */
+#define GSJ_PATH_SORT 4u  /* cfg.sort: thread per query, the reference's pruned
+                             scans of sorted cells, count + fill              */
 
 typedef struct gsj_context gsj_context;
 

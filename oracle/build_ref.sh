@@ -25,7 +25,7 @@ OUT="$HERE/_ref"
 mkdir -p "$OUT"
 JOBS=${JOBS:-4}
 
-# name  GPUNUMDIM NUMINDEXEDDIM DTYPE STAMP REORDER ILP SHORTCIRCUIT QUERYREORDER PRINTNEIGHBORTABLE
+# name  GPUNUMDIM NUMINDEXEDDIM DTYPE STAMP REORDER ILP SHORTCIRCUIT QUERYREORDER PRINTNEIGHBORTABLE [SORT]
 CONFIGS=(
   "d2_plain        2  2 float  0 0 0 0 0 1"
   "d2_plain_f64    2  2 double 0 0 0 0 0 1"
@@ -42,10 +42,13 @@ CONFIGS=(
   "d5_k3_f64_ilp8    5 3 double 0 1 8 0 0 1"
   "d3_k3_f64_ilp2    3 3 double 0 0 2 0 0 1"
   "d5_k3_f32_ilp2_sc 5 3 float  0 1 2 1 1 1"
+  "d2_sort           2 2 float  0 0 0 0 0 1 1"
+  "d3_k2_sort        3 2 float  0 0 0 0 0 1 1"
+  "d5_k3_f64_sort    5 3 double 0 1 2 1 0 1 1"
 )
 
 write_params() {  # $1 dir, then the fields
-  local d=$1 n=$2 k=$3 t=$4 st=$5 ro=$6 ilp=$7 sc=$8 qr=$9 pr=${10}
+  local d=$1 n=$2 k=$3 t=$4 st=$5 ro=$6 ilp=$7 sc=$8 qr=$9 pr=${10} so=${11:-0}
   cat > "$d/params.h" <<EOF
 #define BLOCKSIZE 256
 #define GPUNUMDIM $n
@@ -54,7 +57,7 @@ write_params() {  # $1 dir, then the fields
 #define PRINTNEIGHBORTABLE $pr
 #define STAMP $st
 #define LINEARSTAMP 0
-#define SORT 0
+#define SORT $so
 #define REORDER $ro
 #define ILP $ilp
 #define SHORTCIRCUIT $sc

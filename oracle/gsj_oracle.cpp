@@ -60,6 +60,7 @@ struct orc_cfg {
     uint32_t fold_zero;    // device contraction policy, see DevNode
     uint32_t fuse_left;    // chains acc += d*d
     uint32_t cross_left;   // cross-register sums runningDist[0] += runningDist[j]
+    uint32_t sort;         // SORT (params.h:46): per-cell sorted points, pruned scans
 };
 
 }  // extern "C"
@@ -393,6 +394,35 @@ struct Prepared {
     Grid<T> g;
 };
 
+// SORT (GPU.cu:351-395): each cell's points, in the index's order, sorted by
+// their value in the sort dimension (the first non-indexed dimension, dim 0
+// when every dimension is indexed) with std::sort and the reference's
+// comparator (GPU.cu:51-54); the tie order is std::sort's.
+template <typename T>
+struct key_val_sort {
+    unsigned int pid;
+    T value_at_dim;
+};
+template <typename T>
+bool compareByPointValue(const key_val_sort<T>& a, const key_val_sort<T>& b) {
+    return a.value_at_dim < b.value_at_dim;
+}
+
+inline uint32_t sort_dim_of(uint32_t n, uint32_t k) { return n > k ? k : 0u; }
+
+template <typename T>
+void sort_cells(const T* D, uint32_t n, Grid<T>& g) {
+    const uint32_t sd = sort_dim_of(n, g.k);
+    std::vector<key_val_sort<T>> tmp;
+    for (size_t c = 0; c < g.cellIds.size(); c++) {
+        tmp.clear();
+        for (uint32_t s = g.cellBegin[c]; s < g.cellEnd[c]; s++)
+            tmp.push_back({g.lookup[s], D[(uint64_t)g.lookup[s] * n + sd]});
+        std::sort(tmp.begin(), tmp.end(), compareByPointValue<T>);
+        for (size_t x = 0; x < tmp.size(); x++) g.lookup[g.cellBegin[c] + x] = tmp[x].pid;
+    }
+}
+
 template <typename T>
 void prepare(const T* pts, uint64_t N, uint32_t n, T eps, const orc_cfg& cfg, Prepared<T>& P) {
     P.data.assign(pts, pts + N * n);
@@ -404,6 +434,54 @@ void prepare(const T* pts, uint64_t N, uint32_t n, T eps, const orc_cfg& cfg, Pr
     }
     grid_dims<T>(P.data.data(), N, n, cfg.k, eps, P.g);
     build_index<T>(P.data.data(), N, n, eps, P.g);
+    if (cfg.sort) sort_cells<T>(P.data.data(), n, P.g);
+}
+
+// The candidate positions of one neighbour cell under SORT (kernel.cu:400-467):
+// calls f(position in the cell's sorted points) for each point the reference
+// evaluates.  own0 / nb0: the query's and the cell's coordinate in dim 0.
+template <typename T, typename F>
+void sort_scan(const T* D, uint32_t n, uint32_t k, const std::vector<uint32_t>& lookup, uint32_t begin,
+               uint32_t end, const T* p, T eps, uint32_t own0, uint32_t nb0, F&& f) {
+    if (n == k) {
+        // sortedDim = 0, an indexed dimension: from the side nearer the query,
+        // stop at the first point farther than eps in dim 0
+        const bool mid = own0 == nb0, left = own0 > nb0;
+        const uint32_t len = end - begin;
+        for (uint32_t kk = 0; kk < len; kk++) {
+            const uint32_t pos = left ? len - 1 - kk : kk;
+            const T dv = D[(uint64_t)lookup[begin + pos] * n] - p[0];
+            if (std::abs(dv) > eps && !mid) break;
+            f(pos);
+        }
+        return;
+    }
+    // sortedDim = NUMINDEXEDDIM: the stepping search, then the window
+    const uint32_t sd = k;
+    const int offset = (int)begin;
+    const int length = (int)(end - begin) - 1;
+    auto db = [&](int pos) { return D[(uint64_t)lookup[pos + offset] * n + sd]; };
+    int searchIdx = length / 2;
+    bool lessThan;
+    for (int step = (length + 3) / 4; step > 1; step = (step + 1) / 2) {
+        lessThan = ((p[sd] - db(searchIdx)) >= eps);
+        if (lessThan) {
+            searchIdx += step;
+            if (searchIdx > length) searchIdx = length;
+        } else {
+            searchIdx -= step;
+            if (searchIdx < 0) {
+                searchIdx = 0;
+                step = 0;
+            }
+        }
+    }
+    if (searchIdx > 0 && ((p[sd] - db(searchIdx - 1)) <= eps)) searchIdx--;
+    if (searchIdx > 0 && ((p[sd] - db(searchIdx - 1)) <= eps)) searchIdx--;
+    while (searchIdx <= length && ((db(searchIdx) - p[sd]) < eps)) {
+        f((uint32_t)searchIdx);
+        searchIdx++;
+    }
 }
 
 // Runs the join.  When lists == nullptr only counts are produced.  Symmetric
@@ -440,7 +518,7 @@ int join(const T* pts, uint64_t N, uint32_t n, T eps, const orc_cfg& cfg, uint32
             uint64_t lid = linear_id(idx, g.nCells.data(), g.k);
             int64_t ci = find_cell(g.cellIds, lid);
             if (ci < 0) return;
-            for (uint32_t s = g.cellBegin[ci]; s < g.cellEnd[ci]; s++) {
+            auto eval = [&](uint32_t s) {
                 uint32_t c = g.lookup[s];
                 lc++;
                 if (within<T>(p, D + (uint64_t)c * n, n, eps, cfg)) {
@@ -450,6 +528,12 @@ int join(const T* pts, uint64_t N, uint32_t n, T eps, const orc_cfg& cfg, uint32
                         cnt++;
                     }
                 }
+            };
+            if (cfg.sort) {
+                sort_scan<T>(D, n, g.k, g.lookup, g.cellBegin[ci], g.cellEnd[ci], p, eps, own[0], idx[0],
+                             [&](uint32_t pos) { eval(g.cellBegin[ci] + pos); });
+            } else {
+                for (uint32_t s = g.cellBegin[ci]; s < g.cellEnd[ci]; s++) eval(s);
             }
         };
         for_each_cell(g.k, own, rmin, rmax, cfg.stamp_ref != 0, visit);
@@ -740,8 +824,14 @@ int sample_lists(const T* pts, uint64_t N, uint32_t n, T eps, const orc_cfg& cfg
         auto visit = [&](const uint32_t* idx, bool) {
             int64_t ci = find_cell(g.cellIds, linear_id(idx, g.nCells.data(), g.k));
             if (ci < 0) return;
-            for (uint32_t s = g.cellBegin[ci]; s < g.cellEnd[ci]; s++)
+            auto eval = [&](uint32_t s) {
                 if (within<T>(p, D + (uint64_t)g.lookup[s] * n, n, eps, cfg)) v.push_back(g.lookup[s]);
+            };
+            if (cfg.sort)
+                sort_scan<T>(D, n, g.k, g.lookup, g.cellBegin[ci], g.cellEnd[ci], p, eps, own[0], idx[0],
+                             [&](uint32_t pos) { eval(g.cellBegin[ci] + pos); });
+            else
+                for (uint32_t s = g.cellBegin[ci]; s < g.cellEnd[ci]; s++) eval(s);
         };
         for_each_cell(g.k, own, rmin, rmax, false, visit);
         std::sort(v.begin(), v.end());

@@ -37,6 +37,7 @@ class _Cfg(ctypes.Structure):
         ("fold_zero", ctypes.c_uint32),
         ("fuse_left", ctypes.c_uint32),
         ("cross_left", ctypes.c_uint32),
+        ("sort", ctypes.c_uint32),
     ]
 
 
@@ -55,6 +56,7 @@ class OracleConfig:
     fold_zero: bool | None = None  # None: the pinned policy of the dtype
     fuse_left: bool | None = None
     cross_left: bool | None = None
+    sort: bool = False        # SORT: per-cell sorted points, pruned scans (params.h:46)
 
     def c(self, dtype=np.float32) -> _Cfg:
         fz, fl, xl = pinned_policy(dtype)
@@ -62,7 +64,8 @@ class OracleConfig:
         fl = fl if self.fuse_left is None else self.fuse_left
         xl = xl if self.cross_left is None else self.cross_left
         return _Cfg(self.k, int(self.reorder), self.ilp, int(self.shortcircuit), self.model,
-                    int(self.sc_contract), int(self.stamp_ref), self.nthreads, int(fz), int(fl), int(xl))
+                    int(self.sc_contract), int(self.stamp_ref), self.nthreads, int(fz), int(fl), int(xl),
+                    int(self.sort))
 
 
 def pinned_policy(dtype) -> tuple[bool, bool, bool]:

@@ -53,7 +53,12 @@ PIN_CONFIGS = {
     "d5_k3_f64_ilp8": (5, 3, "float64", True, 8, False, False, 60000, 1.3),
     "d3_k3_f64_ilp2": (3, 3, "float64", False, 2, False, False, 30000, 2.0),
     "d5_k3_f32_ilp2_sc": (5, 3, "float32", True, 2, True, True, 30000, 2.0),
+    "d2_sort": (2, 2, "float32", False, 0, False, False, 40000, 1.0),
+    "d3_k2_sort": (3, 2, "float32", False, 0, False, False, 40000, 1.5),
+    "d5_k3_f64_sort": (5, 3, "float64", True, 2, True, False, 30000, 2.0),
 }
+# configurations built with SORT=1 (params.h:46; oracle/build_ref.sh)
+SORTED = {"d2_sort", "d3_k2_sort", "d5_k3_f64_sort"}
 
 
 def pin_points(name: str) -> np.ndarray:
@@ -98,13 +103,17 @@ def oracle_variants(O, name, pts):
     """Every contraction policy of the device model (see DevNode in
     oracle/gsj_oracle.cpp) plus the host's unfused arithmetic."""
     n, k, dt, reorder, ilp, sc, qr, N, eps = PIN_CONFIGS[name]
+    srt = name in SORTED
     out = {}
     for fz in (False, True):
         for fl in (False, True):
             for xl in (False, True):
                 out[f"fold{int(fz)}_left{int(fl)}_xleft{int(xl)}"] = O.OracleConfig(
-                    k=k, reorder=reorder, ilp=ilp, shortcircuit=sc, fold_zero=fz, fuse_left=fl, cross_left=xl)
-    out["pinned"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc)
+                    k=k, reorder=reorder, ilp=ilp, shortcircuit=sc, fold_zero=fz, fuse_left=fl, cross_left=xl,
+                    sort=srt)
+    out["pinned"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc, sort=srt)
+    if srt:
+        out["unsorted_traversal"] = O.OracleConfig(k=k, reorder=reorder, ilp=ilp, shortcircuit=sc)
     out["host_unfused"] = O.OracleConfig(k=k, reorder=reorder, ilp=0, model=O.MODEL_HOST)
     return out
 
@@ -147,7 +156,7 @@ def main():
         n, k, dt, reorder, ilp, sc, qr, N, eps = spec
         binary = os.path.join(ROOT, "oracle", "_ref", cfgname, "main")
         rec = {"config": cfgname, "N": int(N), "n": n, "k": k, "dtype": dt, "reorder": reorder, "ilp": ilp,
-               "shortcircuit": sc, "query_reorder": qr, "eps": eps}
+               "shortcircuit": sc, "query_reorder": qr, "eps": eps, "sort": name in SORTED}
         if not os.path.exists(binary):
             rec["status"] = "reference binary missing"
             results[name] = rec
@@ -201,12 +210,12 @@ def merge_into_golden(*result_files: str) -> None:
     sorted per-point lists)."""
     path = os.path.join(HERE, "ref_pins.json")
     gold = json.load(open(path)) if os.path.exists(path) else {}
-    keep = ("config", "N", "n", "k", "dtype", "reorder", "ilp", "shortcircuit", "query_reorder", "eps",
+    keep = ("config", "N", "n", "k", "dtype", "reorder", "ilp", "shortcircuit", "query_reorder", "eps", "sort",
             "reference_total", "reference_lists_sha256")
     for f in result_files:
         for name, rec in json.load(open(f)).items():
             if rec.get("status") == "ok":
-                gold[name] = {k: rec[k] for k in keep}
+                gold[name] = {k: rec.get(k, False) for k in keep}
                 gold[name]["gpu_stats_line"] = ", ".join(rec["gpu_stats_line"].split(", ")[2:])
     with open(path, "w") as fh:
         json.dump(gold, fh, indent=1, sort_keys=True)

@@ -42,7 +42,7 @@ def test_oracle_reproduces_reference(oracle, name):
     spec = PINS[name]
     pts = _input(name)
     cfg = oracle.OracleConfig(k=spec["k"], reorder=spec["reorder"], ilp=spec["ilp"],
-                              shortcircuit=spec["shortcircuit"])
+                              shortcircuit=spec["shortcircuit"], sort=spec.get("sort", False))
     counts, _, nbrs = oracle.join_lists(pts, spec["eps"], cfg)
     assert int(counts.sum(dtype=np.uint64)) == spec["reference_total"]
     assert lists_digest(counts, nbrs) == spec["reference_lists_sha256"]
@@ -57,7 +57,8 @@ def test_gpu_reproduces_reference(name, stamp):
     spec = PINS[name]
     pts = _input(name)
     cfg = JoinConfig(indexed_dims=spec["k"], reorder=spec["reorder"], ilp=spec["ilp"],
-                     shortcircuit=spec["shortcircuit"], query_reorder=spec["query_reorder"], stamp=stamp)
+                     shortcircuit=spec["shortcircuit"], query_reorder=spec["query_reorder"], stamp=stamp,
+                     sort=spec.get("sort", False))
     with SelfJoin(0) as sj:
         st = sj.run(pts, spec["eps"], cfg)
         counts, table = sj.counts(), sj.table()
