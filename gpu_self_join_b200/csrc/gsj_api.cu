@@ -379,24 +379,24 @@ int validate(gsj_context* c, const gsj_config& cfg, uint64_t N) {
 }
 
 // ------------------------------------------------------------------ lists ascending
-// Sorts every list of the table ascending (ids below N): a warp per short
-// list, a CTA per long one with a scratch copy of the table.
+// Sorts every list of the table ascending (ids below N): a warp per list up
+// to 256 entries, a CTA bitonic network up to 4096, CTA radix passes with a
+// scratch copy of the table above.
 int sort_table_lists(gsj_context* c, uint32_t* table, const uint64_t* offsets, uint64_t N, uint64_t R) {
     gsj_stats& S = c->stats;
     cudaStream_t st = c->st;
     int nl = 0;
-    GSJ_CUDA(c, sort_short_lists(table, offsets, (uint32_t)N, c->num_sms, &nl, st));
     void* temp = nullptr;
     GSJ_TRY(dev_get(c, c->ptemp, place_temp_bytes(N), (unsigned char**)&temp));
     uint32_t* d_nlong = reinterpret_cast<uint32_t*>(c->misc.p) + 4 * kMaxK + 24;
-    uint32_t nlong = 0;
-    GSJ_CUDA(c, find_long_lists(offsets, (uint32_t)N, temp, d_nlong, &nlong, &nl, st));
+    uint32_t nlong = 0, nvery = 0;
+    GSJ_CUDA(c, sort_short_lists(table, offsets, (uint32_t)N, temp, d_nlong, &nlong, &nvery, c->num_sms, &nl, st));
     if (nlong) {
         uint32_t* scratch = nullptr;
-        GSJ_TRY(dev_get(c, c->table2, R, &scratch));
+        if (nvery) GSJ_TRY(dev_get(c, c->table2, R, &scratch));
         uint32_t id_bits = 1;
         while (id_bits < 32 && ((N - 1) >> id_bits)) id_bits++;
-        GSJ_CUDA(c, sort_long_lists(table, scratch, offsets, temp, nlong, id_bits, c->num_sms, &nl, st));
+        GSJ_CUDA(c, sort_long_lists(table, scratch, offsets, temp, nlong, nvery, id_bits, c->num_sms, &nl, st));
     }
     S.kernel_launches += (uint64_t)nl;
     return GSJ_OK;

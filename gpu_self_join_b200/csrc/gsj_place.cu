@@ -12,7 +12,9 @@
 //   list sort      every list ascending, which also makes the table
 //                  independent of the emission order: a warp per list held in
 //                  registers (bitonic network) up to kWarpSortMax entries, a
-//                  CTA per list (LSD radix passes through a scratch copy) above.
+//                  CTA per list (bitonic network in registers, shuffles and
+//                  shared memory) up to kCtaSortMax, above that a CTA per list
+//                  of LSD radix passes through a scratch copy.
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -26,6 +28,8 @@ namespace {
 
 constexpr unsigned long long kPadKey = ~0ull;  // unused entries of reserved blocks
 constexpr uint32_t kWarpSortMax = 256;         // 8 entries per lane
+constexpr int kCtaSortThreads = 256;
+constexpr uint32_t kCtaSortMax = 4096;         // 16 entries per thread
 constexpr int kBlockSortThreads = 256;
 
 __device__ __forceinline__ unsigned lanemask_lt_p() {
@@ -72,20 +76,64 @@ __global__ void k_pair_place(const unsigned long long* __restrict__ keys, uint64
     }
 }
 
-// Bitonic sort of one list of up to 32*E entries held as E registers per lane
-// (entry r*32 + lane), padded with 0xffffffff; lists whose length lies in
-// (lo, 32*E] are sorted by this instantiation.
+// Bitonic sort of one list of n <= 32*E entries held as E registers per lane
+// (entry r*32 + lane), padded with 0xffffffff.  Called by a whole warp.
 template <int E>
-__global__ void __launch_bounds__(256) k_list_sort_warp(uint32_t* __restrict__ table,
-                                                        const uint64_t* __restrict__ offsets, uint32_t nlists,
-                                                        uint32_t lo) {
+__device__ __forceinline__ void warp_bitonic(uint32_t* __restrict__ list, uint32_t n, int lane) {
+    const unsigned FULL = 0xffffffffu;
+    constexpr uint32_t P = 32u * E;
+    uint32_t v[E];
+#pragma unroll
+    for (int r = 0; r < E; r++) {
+        const uint32_t i = (uint32_t)r * 32u + (uint32_t)lane;
+        v[r] = i < n ? list[i] : 0xffffffffu;
+    }
+#pragma unroll
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+#pragma unroll
+        for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+#pragma unroll
+            for (int r = 0; r < E; r++) {
+                const uint32_t i = (uint32_t)r * 32u + (uint32_t)lane;
+                const bool up = (i & k) == 0u;
+                if (jj >= 32u) {
+                    const int pr = r ^ (int)(jj >> 5);
+                    if (pr > r) {
+                        const uint32_t a = v[r], c = v[pr];
+                        const bool sw = up ? (a > c) : (a < c);
+                        v[r] = sw ? c : a;
+                        v[pr] = sw ? a : c;
+                    }
+                } else {
+                    const uint32_t o = __shfl_xor_sync(FULL, v[r], (int)jj);
+                    const bool lower = (i & jj) == 0u;
+                    v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < E; r++) {
+        const uint32_t i = (uint32_t)r * 32u + (uint32_t)lane;
+        if (i < n) list[i] = v[r];
+    }
+}
+
+// Every list of 2..kWarpSortMax entries sorted by one warp (the network sized
+// to the list: 32, 64, 128 or 256 entries); lists above kWarpSortMax are
+// gathered into long_lists (*nlong, warp-aggregated), those above
+// kCtaSortMax counted in *nvery.
+__global__ void __launch_bounds__(256) k_list_sort_short(uint32_t* __restrict__ table,
+                                                         const uint64_t* __restrict__ offsets, uint32_t nlists,
+                                                         uint32_t* __restrict__ long_lists,
+                                                         uint32_t* __restrict__ nlong) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt_p();
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    constexpr uint32_t P = 32u * E;
     for (uint32_t l0 = gw * 32u; l0 < nlists; l0 += nw * 32u) {
-        // the lengths of 32 consecutive lists, then the lists of this size class one by one
+        // the lengths of 32 consecutive lists, then the short ones one by one
         const uint32_t li = l0 + (uint32_t)lane;
         uint64_t b = 0, e = 0;
         if (li < nlists) {
@@ -93,52 +141,101 @@ __global__ void __launch_bounds__(256) k_list_sort_warp(uint32_t* __restrict__ t
             e = offsets[li + 1];
         }
         const uint64_t len = e - b;
-        unsigned mine = __ballot_sync(FULL, li < nlists && len > lo && len <= P);
+        const unsigned lng = __ballot_sync(FULL, len > kWarpSortMax);
+        if (lng) {
+            uint32_t at = 0;
+            if (lane == 0) at = atomicAdd(nlong, (uint32_t)__popc(lng));
+            at = __shfl_sync(FULL, at, 0);
+            if ((lng >> lane) & 1u) long_lists[at + (uint32_t)__popc(lng & lt)] = li;
+            const unsigned vl = __ballot_sync(FULL, len > kCtaSortMax);
+            if (vl && lane == 0) atomicAdd(nlong + 1, (uint32_t)__popc(vl));
+        }
+        unsigned mine = __ballot_sync(FULL, len > 1u && len <= kWarpSortMax);
         while (mine) {
             const int j = __ffs(mine) - 1;
             mine &= mine - 1u;
-            const uint64_t base = __shfl_sync(FULL, b, j);
+            uint32_t* list = table + __shfl_sync(FULL, b, j);
             const uint32_t n = (uint32_t)__shfl_sync(FULL, len, j);
-            uint32_t v[E];
-#pragma unroll
-            for (int r = 0; r < E; r++) {
-                const uint32_t i = (uint32_t)r * 32u + (uint32_t)lane;
-                v[r] = i < n ? table[base + i] : 0xffffffffu;
-            }
-#pragma unroll
-            for (uint32_t k = 2; k <= P; k <<= 1) {
-#pragma unroll
-                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
-#pragma unroll
-                    for (int r = 0; r < E; r++) {
-                        const uint32_t i = (uint32_t)r * 32u + (uint32_t)lane;
-                        const bool up = (i & k) == 0u;
-                        if (jj >= 32u) {
-                            const int pr = r ^ (int)(jj >> 5);
-                            if (pr > r) {
-                                const uint32_t a = v[r], c = v[pr];
-                                const bool sw = up ? (a > c) : (a < c);
-                                v[r] = sw ? c : a;
-                                v[pr] = sw ? a : c;
-                            }
-                        } else {
-                            const uint32_t o = __shfl_xor_sync(FULL, v[r], (int)jj);
-                            const bool lower = (i & jj) == 0u;
-                            v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < E; r++) {
-                const uint32_t i = (uint32_t)r * 32u + (uint32_t)lane;
-                if (i < n) table[base + i] = v[r];
-            }
+            if (n <= 32u) warp_bitonic<1>(list, n, lane);
+            else if (n <= 64u) warp_bitonic<2>(list, n, lane);
+            else if (n <= 128u) warp_bitonic<4>(list, n, lane);
+            else warp_bitonic<8>(list, n, lane);
         }
     }
 }
 
-// One CTA per list longer than kWarpSortMax: LSD radix passes of 8 bits over
+// Bitonic sort of one list of n <= 256*E entries by the whole CTA
+// (kCtaSortThreads threads), entry r*256 + t in register r of thread t.
+// Exchange distances below 32 use shuffles; the others go through one of two
+// shared-memory buffers (alternated by *buf, so each such stage needs one
+// barrier: a buffer is rewritten only after every thread passed the barrier
+// that followed its last read).
+template <int E>
+__device__ __forceinline__ void cta_bitonic(uint32_t* __restrict__ list, uint32_t n, uint32_t (*sb)[kCtaSortMax],
+                                            int& buf) {
+    const unsigned FULL = 0xffffffffu;
+    const uint32_t t = threadIdx.x;
+    constexpr uint32_t P = (uint32_t)kCtaSortThreads * E;
+    uint32_t v[E];
+#pragma unroll
+    for (int r = 0; r < E; r++) {
+        const uint32_t i = (uint32_t)r * kCtaSortThreads + t;
+        v[r] = i < n ? list[i] : 0xffffffffu;
+    }
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32u) {
+                uint32_t* s = sb[buf];
+                buf ^= 1;
+#pragma unroll
+                for (int r = 0; r < E; r++) s[(uint32_t)r * kCtaSortThreads + t] = v[r];
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < E; r++) {
+                    const uint32_t i = (uint32_t)r * kCtaSortThreads + t;
+                    const uint32_t o = s[i ^ j];
+                    const bool up = (i & k) == 0u, lower = (i & j) == 0u;
+                    v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < E; r++) {
+                    const uint32_t i = (uint32_t)r * kCtaSortThreads + t;
+                    const uint32_t o = __shfl_xor_sync(FULL, v[r], (int)j);
+                    const bool up = (i & k) == 0u, lower = (i & j) == 0u;
+                    v[r] = (lower == up) ? min(v[r], o) : max(v[r], o);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < E; r++) {
+        const uint32_t i = (uint32_t)r * kCtaSortThreads + t;
+        if (i < n) list[i] = v[r];
+    }
+}
+
+// A CTA per list of kWarpSortMax+1 .. kCtaSortMax entries (longer lists are
+// left to k_list_sort_block).
+__global__ void __launch_bounds__(kCtaSortThreads) k_list_sort_cta(uint32_t* __restrict__ table,
+                                                                   const uint64_t* __restrict__ offsets,
+                                                                   const uint32_t* __restrict__ long_lists,
+                                                                   uint32_t nlong) {
+    __shared__ uint32_t sb[2][kCtaSortMax];
+    int buf = 0;
+    for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x) {
+        const uint32_t l = long_lists[li];
+        const uint64_t b = offsets[l];
+        const uint32_t n = (uint32_t)(offsets[l + 1] - b);
+        if (n > kCtaSortMax) continue;
+        if (n <= 512u) cta_bitonic<2>(table + b, n, sb, buf);
+        else if (n <= 1024u) cta_bitonic<4>(table + b, n, sb, buf);
+        else if (n <= 2048u) cta_bitonic<8>(table + b, n, sb, buf);
+        else cta_bitonic<16>(table + b, n, sb, buf);
+    }
+}
+
+// One CTA per list longer than kCtaSortMax: LSD radix passes of 8 bits over
 // the list's entries (ids below 2^bits), alternating between the table and
 // the same range of `scratch`; the pass count is even, so the sorted list ends
 // in the table.  Each pass: a digit histogram of the whole list, then its
@@ -158,6 +255,7 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_list_sort_block(uint32_t*
         const uint32_t l = long_lists[li];
         const uint64_t b = offsets[l];
         const uint32_t n = (uint32_t)(offsets[l + 1] - b);
+        if (n <= kCtaSortMax) continue;  // block-uniform: sorted by k_list_sort_cta
         uint32_t* src = table + b;
         uint32_t* dst = scratch + b;
         for (int p = 0; p < passes; p++) {
@@ -206,12 +304,6 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_list_sort_block(uint32_t*
     }
 }
 
-__global__ void k_long_lists(const uint64_t* __restrict__ offsets, uint32_t nlists, uint32_t lo,
-                             uint32_t* __restrict__ out, uint32_t* __restrict__ nout) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nlists && offsets[i + 1] - offsets[i] > lo) out[atomicAdd(nout, 1u)] = i;
-}
-
 inline unsigned grid_for(uint64_t n, unsigned t, uint64_t cap) {
     uint64_t b = (n + t - 1) / t;
     if (b > cap) b = cap;
@@ -224,40 +316,43 @@ size_t place_temp_bytes(uint64_t nlists) {
     return (nlists + 64) * sizeof(uint32_t) + scan_u32_u64_temp_bytes(nlists) + 256;
 }
 
-cudaError_t sort_short_lists(uint32_t* table, const uint64_t* offsets, uint32_t nlists, int num_sms, int* launches,
+cudaError_t sort_short_lists(uint32_t* table, const uint64_t* offsets, uint32_t nlists, void* temp,
+                             uint32_t* d_nlong, uint32_t* h_nlong, uint32_t* h_nvery, int num_sms, int* launches,
                              cudaStream_t st) {
+    *h_nlong = *h_nvery = 0;
     if (nlists == 0) return cudaSuccess;
-    const unsigned g = grid_for((uint64_t)nlists * 32u, 256, (uint64_t)num_sms * 64);
-    k_list_sort_warp<1><<<g, 256, 0, st>>>(table, offsets, nlists, 1u);
-    k_list_sort_warp<2><<<g, 256, 0, st>>>(table, offsets, nlists, 32u);
-    k_list_sort_warp<4><<<g, 256, 0, st>>>(table, offsets, nlists, 64u);
-    k_list_sort_warp<8><<<g, 256, 0, st>>>(table, offsets, nlists, 128u);
-    if (launches) *launches += 4;
-    return cudaGetLastError();
-}
-
-cudaError_t find_long_lists(const uint64_t* offsets, uint32_t nlists, void* temp, uint32_t* d_nlong,
-                            uint32_t* h_nlong, int* launches, cudaStream_t st) {
-    *h_nlong = 0;
-    if (nlists == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(d_nlong, 0, sizeof(uint32_t), st);
+    cudaError_t e = cudaMemsetAsync(d_nlong, 0, 2 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    k_long_lists<<<grid_for(nlists, 256, ~0ull), 256, 0, st>>>(offsets, nlists, kWarpSortMax,
-                                                              static_cast<uint32_t*>(temp), d_nlong);
+    const unsigned g = grid_for((uint64_t)nlists, 256, (uint64_t)num_sms * 64);
+    k_list_sort_short<<<g, 256, 0, st>>>(table, offsets, nlists, static_cast<uint32_t*>(temp), d_nlong);
     if (launches) *launches += 1;
-    e = cudaMemcpyAsync(h_nlong, d_nlong, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    uint32_t h[2];
+    e = cudaMemcpyAsync(h, d_nlong, sizeof(h), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return e;
-    return cudaStreamSynchronize(st);
+    e = cudaStreamSynchronize(st);
+    *h_nlong = h[0];
+    *h_nvery = h[1];
+    return e;
 }
 
 cudaError_t sort_long_lists(uint32_t* table, uint32_t* scratch, const uint64_t* offsets, const void* temp,
-                            uint32_t nlong, uint32_t id_bits, int num_sms, int* launches, cudaStream_t st) {
+                            uint32_t nlong, uint32_t nvery, uint32_t id_bits, int num_sms, int* launches,
+                            cudaStream_t st) {
     if (nlong == 0) return cudaSuccess;
-    int passes = (int)((id_bits + 7u) / 8u);
-    passes += passes & 1;  // even: the sorted list ends in the table
-    k_list_sort_block<<<grid_for(nlong, 1, (uint64_t)num_sms * 8), kBlockSortThreads, 0, st>>>(
-        table, scratch, offsets, static_cast<const uint32_t*>(temp), nlong, passes);
-    if (launches) *launches += 1;
+    const uint32_t* ll = static_cast<const uint32_t*>(temp);
+    if (nlong > nvery) {
+        k_list_sort_cta<<<grid_for(nlong - nvery, 1, (uint64_t)num_sms * 6), kCtaSortThreads, 0, st>>>(
+            table, offsets, ll, nlong);
+        if (launches) *launches += 1;
+    }
+    if (nvery) {
+        if (!scratch) return cudaErrorInvalidValue;
+        int passes = (int)((id_bits + 7u) / 8u);
+        passes += passes & 1;  // even: the sorted list ends in the table
+        k_list_sort_block<<<grid_for(nvery, 1, (uint64_t)num_sms * 8), kBlockSortThreads, 0, st>>>(
+            table, scratch, offsets, ll, nlong, passes);
+        if (launches) *launches += 1;
+    }
     return cudaGetLastError();
 }
 

@@ -56,14 +56,36 @@ PIN_CONFIGS = {
     "d2_sort": (2, 2, "float32", False, 0, False, False, 40000, 1.0),
     "d3_k2_sort": (3, 2, "float32", False, 0, False, False, 40000, 1.5),
     "d5_k3_f64_sort": (5, 3, "float64", True, 2, True, False, 30000, 2.0),
+    "d3_k2_sort_gap": (3, 2, "float32", False, 0, False, False, 40000, 0.5),
 }
 # configurations built with SORT=1 (params.h:46; oracle/build_ref.sh)
-SORTED = {"d2_sort", "d3_k2_sort", "d5_k3_f64_sort"}
+SORTED = {"d2_sort", "d3_k2_sort", "d5_k3_f64_sort", "d3_k2_sort_gap"}
+# pins that run another pin's reference build
+BUILD_OF = {"d3_k2_sort_gap": "d3_k2_sort"}
+
+
+def gap_points(name: str) -> np.ndarray:
+    """Pairs of points equal in the indexed dimensions and exactly eps apart
+    in the sort dimension (values are multiples of eps, exact in binary): the
+    pruned window's strict `< eps` (kernel.cu:461) drops the partner above
+    the query, while the full scan reports both directions."""
+    n, k, dt, _, _, _, _, N, eps = PIN_CONFIGS[name]
+    seed = int.from_bytes(hashlib.sha256(name.encode()).digest()[:4], "little")
+    rng = np.random.default_rng(seed)
+    m = N // 2
+    base = rng.uniform(0, 40 * eps, size=(m, n))
+    base[:, k] = rng.integers(0, 80, m) * eps
+    partner = base.copy()
+    partner[:, k] += eps
+    pts = np.concatenate([base, partner]).astype(dt)
+    return pts[rng.permutation(N)]
 
 
 def pin_points(name: str) -> np.ndarray:
     """Seeded input of a pin configuration: clustered points plus partners
     placed at distance eps (computed in float64, then rounded)."""
+    if name.endswith("_gap"):
+        return gap_points(name)
     n, k, dt, _, _, _, _, N, eps = PIN_CONFIGS[name]
     seed = int.from_bytes(hashlib.sha256(name.encode()).digest()[:4], "little")
     rng = np.random.default_rng(seed)
@@ -151,7 +173,7 @@ def main():
             spec = (2, 2, "float32", False, 0, False, False, pts.shape[0], 1.0)
             PIN_CONFIGS["test_dat"] = spec
         else:
-            cfgname, pts = name, pin_points(name)
+            cfgname, pts = BUILD_OF.get(name, name), pin_points(name)
             spec = PIN_CONFIGS[name]
         n, k, dt, reorder, ilp, sc, qr, N, eps = spec
         binary = os.path.join(ROOT, "oracle", "_ref", cfgname, "main")

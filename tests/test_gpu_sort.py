@@ -70,3 +70,18 @@ def test_sort_host_result(oracle):
 def test_sort_tiny(oracle, N):
     pts = np.arange(N * 3, dtype=np.float32).reshape(N, 3) * 0.1
     check(oracle, pts, 1.0, 2)
+
+
+def test_sort_exact_gap_window(oracle):
+    # partners exactly eps apart in the sort dimension: the strict window of
+    # the pruned scan drops one direction, the GPU drops the same pairs
+    rng = np.random.default_rng(31)
+    m, eps = 10000, 0.5
+    base = rng.uniform(0, 20, size=(m, 3))
+    base[:, 2] = rng.integers(0, 80, m) * eps
+    partner = base.copy()
+    partner[:, 2] += eps
+    pts = np.concatenate([base, partner]).astype(np.float32)[rng.permutation(2 * m)]
+    full, _, _ = oracle.join_counts(pts, eps, oracle.OracleConfig(k=2))
+    st = check(oracle, pts, eps, 2)
+    assert st["total_pairs"] < int(full.sum())
