@@ -35,6 +35,18 @@ def test_fixture_covers_both_precisions_and_models():
     assert {v["ilp"] for v in PINS.values()} >= {0, 2, 4, 8}
     assert {v["shortcircuit"] for v in PINS.values()} == {False, True}
     assert PINS["test_dat"]["reference_total"] == 27982028
+    # SORT=1 builds (params.h:46), both sort-dimension cases, and one input on
+    # which the pruned window drops pairs that the full traversal reports
+    srt = {k: v for k, v in PINS.items() if v.get("sort")}
+    assert {v["n"] == v["k"] for v in srt.values()} == {True, False}
+    assert "d3_k2_sort_gap" in srt
+
+
+def test_sort_gap_pin_differs_from_full_traversal(oracle):
+    spec = PINS["d3_k2_sort_gap"]
+    pts = _input("d3_k2_sort_gap")
+    _, full, _ = oracle.join_counts(pts, spec["eps"], oracle.OracleConfig(k=spec["k"]))
+    assert spec["reference_total"] < full
 
 
 @pytest.mark.parametrize("name", sorted(PINS))
