@@ -390,13 +390,15 @@ int sort_table_lists(gsj_context* c, uint32_t* table, const uint64_t* offsets, u
     GSJ_TRY(dev_get(c, c->ptemp, place_temp_bytes(N), (unsigned char**)&temp));
     uint32_t* d_nlong = reinterpret_cast<uint32_t*>(c->misc.p) + 4 * kMaxK + 24;
     uint32_t nlong = 0, nvery = 0;
-    GSJ_CUDA(c, sort_short_lists(table, offsets, (uint32_t)N, temp, d_nlong, &nlong, &nvery, c->num_sms, &nl, st));
+    GSJ_CUDA(c, sort_short_lists<uint64_t>(table, offsets, (uint32_t)N, 1u, temp, d_nlong, &nlong, &nvery,
+                                           c->num_sms, &nl, st));
     if (nlong) {
         uint32_t* scratch = nullptr;
         if (nvery) GSJ_TRY(dev_get(c, c->table2, R, &scratch));
         uint32_t id_bits = 1;
         while (id_bits < 32 && ((N - 1) >> id_bits)) id_bits++;
-        GSJ_CUDA(c, sort_long_lists(table, scratch, offsets, temp, nlong, nvery, id_bits, c->num_sms, &nl, st));
+        GSJ_CUDA(c, sort_long_lists<uint64_t>(table, scratch, offsets, temp, nlong, nvery, id_bits, c->num_sms, &nl,
+                                              st));
     }
     S.kernel_launches += (uint64_t)nl;
     return GSJ_OK;
@@ -1011,8 +1013,12 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     GSJ_TRY(dev_get(c, c->minarr, k, &d_min));
     GSJ_CUDA(c, cudaMemcpyAsync(d_min, minArr.data(), k * sizeof(T), cudaMemcpyHostToDevice, st));
 
-    // ---- cell keys + radix sort (subsystem (a)): points ordered by cell, ties
-    // by point id (a stable sort of keys generated in point-id order)
+    // ---- points ordered by cell, ties by point id (subsystem (a)).  Dense grids
+    // (a slot-prefix table over every linear cell id): a counting sort - cell
+    // ids with per-cell counts and arrival ranks, the scan of the counts (which
+    // is the slot-prefix table), a scatter, then the ids of every cell sorted
+    // ascending.  Other grids: a stable LSD radix sort of keys generated in
+    // point-id order.
     uint64_t *keys = nullptr, *keys2 = nullptr;
     uint32_t *vals = nullptr, *ids = nullptr;
     GSJ_TRY(dev_get(c, c->keys, N, &keys));
@@ -1022,22 +1028,42 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     int bits = 1;
     while (bits < 64 && (totalCells - 1) >> bits) bits++;
     const bool key32 = bits <= 32;
+    const uint64_t dense_limit = std::max<uint64_t>(1u << 24, 8ull * N);
+    const bool dense = totalCells <= dense_limit && totalCells < (1ull << 30);
     void* temp = nullptr;
-    GSJ_TRY(dev_get(c, c->temp, std::max(radix_sort_temp_bytes(N), runs_temp_bytes(N)), (unsigned char**)&temp));
+    GSJ_TRY(dev_get(c, c->temp,
+                    std::max({radix_sort_temp_bytes(N), runs_temp_bytes(N),
+                              dense ? scan_u32_u64_temp_bytes(totalCells) : (size_t)0}),
+                    (unsigned char**)&temp));
     bool in_alt = false;
     int nl = 0;
+    uint32_t *ds = nullptr, *dcnt = nullptr;
+    // the number of non-empty cells (word 0) and the out-of-range flag of the
+    // cell keys (word 1)
+    uint32_t* d_nruns = reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK);
+    GSJ_CUDA(c, cudaMemsetAsync(d_nruns, 0, 2 * sizeof(uint32_t), st));
     S.kernel_launches += 1;
-    if (key32) {
+    if (dense) {
+        GSJ_TRY(dev_get(c, c->dense, totalCells + 1, &ds));
+        GSJ_TRY(dev_get(c, c->dcnt, totalCells + 1, &dcnt));
+        GSJ_CUDA(c, cudaMemsetAsync(dcnt, 0, (totalCells + 1) * sizeof(uint32_t), st));
+        uint32_t* k32 = reinterpret_cast<uint32_t*>(keys);
+        GSJ_CUDA(c, launch_cell_keys_count<T>(d_in, N, n, d_perm, g, d_min, eps, k32, dcnt, vals, d_nruns + 1, st));
+        // ds[L] = points in cells below L (ds[totalCells] = N)
+        S.kernel_launches += 4;
+        GSJ_CUDA(c, scan_u32_u32(dcnt, ds, totalCells, temp, st));
+        GSJ_CUDA(c, launch_count_scatter(k32, vals, ds, N, reinterpret_cast<uint32_t*>(keys2), ids, st));
+    } else if (key32) {
         uint32_t* k32 = reinterpret_cast<uint32_t*>(keys);
         uint32_t* k32b = reinterpret_cast<uint32_t*>(keys2);
-        GSJ_CUDA(c, (launch_cell_keys<T, uint32_t>(d_in, N, n, d_perm, g, d_min, eps, k32, vals, st)));
+        GSJ_CUDA(c, (launch_cell_keys<T, uint32_t>(d_in, N, n, d_perm, g, d_min, eps, k32, vals, d_nruns + 1, st)));
         GSJ_CUDA(c, radix_sort<uint32_t>(k32, k32b, vals, ids, N, 0, bits, temp, &in_alt, &nl, st));
     } else {
-        GSJ_CUDA(c, (launch_cell_keys<T, uint64_t>(d_in, N, n, d_perm, g, d_min, eps, keys, vals, st)));
+        GSJ_CUDA(c, (launch_cell_keys<T, uint64_t>(d_in, N, n, d_perm, g, d_min, eps, keys, vals, d_nruns + 1, st)));
         GSJ_CUDA(c, radix_sort<uint64_t>(keys, keys2, vals, ids, N, 0, bits, temp, &in_alt, &nl, st));
     }
     S.kernel_launches += (uint64_t)nl;
-    if (!in_alt) {
+    if (!dense && !in_alt) {
         // an even number of passes (or none) leaves the result in the first buffers
         std::swap(c->keys, c->keys2);
         std::swap(c->vals, c->ids);
@@ -1047,19 +1073,43 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
 
     // ---- runs of equal keys = non-empty cells: cell_key[M], cell_start[M+1]
     uint64_t* cell_key = nullptr;
-    uint32_t *cell_start = nullptr, *d_nruns = nullptr;
+    uint32_t* cell_start = nullptr;
     GSJ_TRY(dev_get(c, c->cell_key, N, &cell_key));
     GSJ_TRY(dev_get(c, c->cell_start, N + 1, &cell_start));
-    d_nruns = reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK);
     S.kernel_launches += 5;
     if (key32)
         GSJ_CUDA(c, run_length<uint32_t>(reinterpret_cast<const uint32_t*>(keys2), N, cell_key, cell_start, d_nruns,
                                          temp, st));
     else
         GSJ_CUDA(c, run_length<uint64_t>(keys2, N, cell_key, cell_start, d_nruns, temp, st));
-    uint32_t M = 0;
-    GSJ_TRY(d2h_small(c, &M, d_nruns, 1));
+    uint32_t runs[2] = {0, 0};
+    GSJ_TRY(d2h_small(c, runs, d_nruns, 2));
+    if (runs[1])
+        return fail(c, GSJ_ERR_INVALID,
+                    "a coordinate maps to the grid's extent (epsilon below the resolution of the data's type)");
+    const uint32_t M = runs[0];
     S.nonempty_cells = M;
+    if (dense && N > 1) {
+        // counting sort: each cell's ids ascending (small cells one thread each,
+        // larger ones by the list sorts; the rank buffer is free as scratch)
+        constexpr uint32_t kSmallCell = 16;
+        S.kernel_launches += 2;
+        GSJ_CUDA(c, launch_cell_ids_small(ids, cell_start, M, kSmallCell, st));
+        void* ptemp = nullptr;
+        GSJ_TRY(dev_get(c, c->ptemp, place_temp_bytes(M), (unsigned char**)&ptemp));
+        uint32_t* d_nlong = reinterpret_cast<uint32_t*>(c->misc.p) + 4 * kMaxK + 24;
+        uint32_t nlong = 0, nvery = 0;
+        int nls = 0;
+        GSJ_CUDA(c, sort_short_lists<uint32_t>(ids, cell_start, M, kSmallCell, ptemp, d_nlong, &nlong, &nvery,
+                                               c->num_sms, &nls, st));
+        if (nlong) {
+            uint32_t id_bits = 1;
+            while (id_bits < 32 && ((N - 1) >> id_bits)) id_bits++;
+            GSJ_CUDA(c, sort_long_lists<uint32_t>(ids, vals, cell_start, ptemp, nlong, nvery, id_bits, c->num_sms,
+                                                  &nls, st));
+        }
+        S.kernel_launches += (uint64_t)nls;
+    }
 
     // ---- SORT (GPU.cu:351-395): each cell's points ordered by their value in the
     // sort dimension with std::sort and the reference's comparator, on the host
@@ -1102,31 +1152,19 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     // ---- cell lookup: on dense grids a slot-prefix table over every linear
     // cell id (cell L holds slots [ds[L], ds[L+1])), else a hash table of the
     // non-empty cells
-    uint32_t *ds = nullptr, *dcnt = nullptr;
+    // (dense grids: ds was built with the counting sort)
     unsigned long long* hkeys = nullptr;
     uint32_t* hvals = nullptr;
     uint64_t hmask = 0;
-    const uint64_t dense_limit = std::max<uint64_t>(1u << 24, 8ull * N);
-    const bool dense = totalCells <= dense_limit && totalCells < (1ull << 30);
-    if (dense) {
-        GSJ_TRY(dev_get(c, c->dense, totalCells + 1, &ds));
-        GSJ_TRY(dev_get(c, c->dcnt, totalCells + 1, &dcnt));
-        GSJ_CUDA(c, cudaMemsetAsync(dcnt, 0, (totalCells + 1) * sizeof(uint32_t), st));
-    } else {
+    if (!dense) {
         uint64_t hcap = 1024;
         while (hcap < 2ull * M) hcap <<= 1;
         hmask = hcap - 1;
         GSJ_TRY(dev_get(c, c->hkeys, hcap, &hkeys));
         GSJ_TRY(dev_get(c, c->hvals, hcap, &hvals));
         GSJ_CUDA(c, cudaMemsetAsync(hkeys, 0xff, hcap * sizeof(unsigned long long), st));
-    }
-    S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, M, dcnt, hkeys, hvals, hmask, st));
-    if (dense) {
-        // the slot-prefix table: ds[L] = points in cells below L (ds[totalCells] = N)
-        GSJ_TRY(dev_get(c, c->temp, scan_u32_u64_temp_bytes(totalCells), (unsigned char**)&temp));
-        S.kernel_launches += 3;
-        GSJ_CUDA(c, scan_u32_u32(dcnt, ds, totalCells, temp, st));
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, M, nullptr, hkeys, hvals, hmask, st));
     }
     // Dense low-dimensional grids use the row-range traversal driven by a
     // per-cell plan of neighbour-row slot ranges.

@@ -143,13 +143,26 @@ __device__ __forceinline__ unsigned lanemask_lt_q() {
 
 // Queries: the slots qslots[0 .. nq) (all slots 0 .. nq-1 when qslots is
 // null); the list of point id i goes to a.table[offsets[i] - base].
+// Per-query parameters of the fill, staged in shared memory by the lane that
+// loaded them and read back by the whole warp (one broadcast per 16 bytes).
+template <int NR>
+struct alignas(16) FillQuery {
+    unsigned long long dst;  // list place in the table (relative to the batch base)
+    unsigned long long bo;   // first mask word
+    uint32_t cnt, nw;        // list length, mask words
+    uint32_t lo[NR];         // first slot of each candidate row
+    uint32_t pre[NR];        // candidates before each row
+};
+
 template <int NR>
 __global__ void __launch_bounds__(256) k_rows_fill(const JoinArgs<float> a, const uint32_t* __restrict__ slot_cell,
                                                    const uint64_t* __restrict__ bitoff,
                                                    const uint32_t* __restrict__ bits,
                                                    const uint32_t* __restrict__ qslots, uint32_t nq, uint64_t base) {
+    __shared__ FillQuery<NR> qp[8][32];  // blockDim.x <= 256
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    FillQuery<NR>* wq = qp[threadIdx.x >> 5];
     const unsigned lt = lanemask_lt_q();
     uint32_t cur = __shfl_sync(FULL, claim32(a.work_counter, lane), 0);
     while (cur < nq) {
@@ -157,49 +170,39 @@ __global__ void __launch_bounds__(256) k_rows_fill(const JoinArgs<float> a, cons
         const uint32_t j = cur + (uint32_t)lane;
         const uint32_t nv = min(32u, nq - cur);
         // lane j: query j's list length, mask words, list place and candidate rows
-        uint32_t cnt = 0, nw = 0;
-        uint64_t bo = 0;
-        unsigned long long dst = 0;
-        uint32_t lo[NR], pre[NR];
-#pragma unroll
-        for (int r = 0; r < NR; r++) lo[r] = pre[r] = 0u;
+        FillQuery<NR> f{};
         if (j < nq) {
             const uint32_t s = qslots ? qslots[j] : j;
-            cnt = a.fwd_cnt[s];
-            bo = bitoff[s];
-            nw = (uint32_t)(bitoff[s + 1] - bo);
-            dst = a.offsets[a.ids[s]] - base;
-            if (dst + cnt > a.table_cap) {
+            f.cnt = a.fwd_cnt[s];
+            f.bo = bitoff[s];
+            f.nw = (uint32_t)(bitoff[s + 1] - f.bo);
+            f.dst = a.offsets[a.ids[s]] - base;
+            if (f.dst + f.cnt > a.table_cap) {
                 *a.err_flag = 1u;
-                cnt = 0u;
+                f.cnt = 0u;
             }
             const uint32_t cell = slot_cell[s];
             uint32_t p = 0;
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 const uint2 e = a.plan[(size_t)cell * NR + r];
-                lo[r] = e.x;
-                pre[r] = p;
+                f.lo[r] = e.x;
+                f.pre[r] = p;
                 p += e.y;
             }
         }
+        __syncwarp();  // the previous chunk's reads of wq are done
+        wq[lane] = f;
+        __syncwarp();
         for (uint32_t qi = 0; qi < nv; qi++) {
-            const uint32_t cq = __shfl_sync(FULL, cnt, qi);
-            if (cq == 0u) continue;
-            const unsigned long long dq = __shfl_sync(FULL, dst, qi);
-            const unsigned long long bq = __shfl_sync(FULL, bo, qi);
-            const uint32_t nwq = __shfl_sync(FULL, nw, qi);
-            uint32_t lq[NR], pq[NR];
-#pragma unroll
-            for (int r = 0; r < NR; r++) {
-                lq[r] = __shfl_sync(FULL, lo[r], qi);
-                pq[r] = __shfl_sync(FULL, pre[r], qi);
-            }
-            uint32_t* list = a.table + dq;
+            const FillQuery<NR> q = wq[qi];
+            if (q.cnt == 0u) continue;
+            uint32_t* list = a.table + q.dst;
+            const uint32_t* qb = bits + q.bo;
             uint32_t run = 0;  // entries of the list written so far
-            for (uint32_t t0 = 0; t0 < nwq && run < cq; t0 += 32u) {
-                const uint32_t myw = (t0 + (uint32_t)lane < nwq) ? bits[bq + t0 + lane] : 0u;
-                const uint32_t tn = min(32u, nwq - t0);
+            for (uint32_t t0 = 0; t0 < q.nw && run < q.cnt; t0 += 32u) {
+                const uint32_t myw = (t0 + (uint32_t)lane < q.nw) ? qb[t0 + lane] : 0u;
+                const uint32_t tn = min(32u, q.nw - t0);
                 // two mask words (64 candidates) per step
                 for (uint32_t tt = 0; tt < tn; tt += 2u) {
                     const uint32_t w0 = __shfl_sync(FULL, myw, tt);
@@ -209,18 +212,18 @@ __global__ void __launch_bounds__(256) k_rows_fill(const JoinArgs<float> a, cons
                     const uint32_t p0 = (uint32_t)__popc(w0);
                     const uint32_t f0 = (t0 + tt) * 32u + (uint32_t)lane;
                     if ((w0 >> lane) & 1u) {
-                        uint32_t st = lq[0] + f0;
+                        uint32_t st = q.lo[0] + f0;
 #pragma unroll
                         for (int r = 1; r < NR; r++)
-                            if (f0 >= pq[r]) st = lq[r] + (f0 - pq[r]);
+                            if (f0 >= q.pre[r]) st = q.lo[r] + (f0 - q.pre[r]);
                         list[run + (uint32_t)__popc(w0 & lt)] = a.ids[st];
                     }
                     if ((w1 >> lane) & 1u) {
                         const uint32_t f1 = f0 + 32u;
-                        uint32_t st = lq[0] + f1;
+                        uint32_t st = q.lo[0] + f1;
 #pragma unroll
                         for (int r = 1; r < NR; r++)
-                            if (f1 >= pq[r]) st = lq[r] + (f1 - pq[r]);
+                            if (f1 >= q.pre[r]) st = q.lo[r] + (f1 - q.pre[r]);
                         list[run + p0 + (uint32_t)__popc(w1 & lt)] = a.ids[st];
                     }
                     run += p0 + (uint32_t)__popc(w1);

@@ -119,13 +119,15 @@ __device__ __forceinline__ void warp_bitonic(uint32_t* __restrict__ list, uint32
     }
 }
 
-// Every list of 2..kWarpSortMax entries sorted by one warp (the network sized
-// to the list: 32, 64, 128 or 256 entries); lists above kWarpSortMax are
-// gathered into long_lists (*nlong, warp-aggregated), those above
-// kCtaSortMax counted in *nvery.
+// Every list of min_len+1..kWarpSortMax entries sorted by one warp (the
+// network sized to the list: 32, 64, 128 or 256 entries); lists above
+// kWarpSortMax are gathered into long_lists (*nlong, warp-aggregated), those
+// above kCtaSortMax counted in *nvery.  List l: table[offsets[l] ..
+// offsets[l+1]).
+template <typename OffT>
 __global__ void __launch_bounds__(256) k_list_sort_short(uint32_t* __restrict__ table,
-                                                         const uint64_t* __restrict__ offsets, uint32_t nlists,
-                                                         uint32_t* __restrict__ long_lists,
+                                                         const OffT* __restrict__ offsets, uint32_t nlists,
+                                                         uint32_t min_len, uint32_t* __restrict__ long_lists,
                                                          uint32_t* __restrict__ nlong) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -137,8 +139,8 @@ __global__ void __launch_bounds__(256) k_list_sort_short(uint32_t* __restrict__ 
         const uint32_t li = l0 + (uint32_t)lane;
         uint64_t b = 0, e = 0;
         if (li < nlists) {
-            b = offsets[li];
-            e = offsets[li + 1];
+            b = (uint64_t)offsets[li];
+            e = (uint64_t)offsets[li + 1];
         }
         const uint64_t len = e - b;
         const unsigned lng = __ballot_sync(FULL, len > kWarpSortMax);
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(256) k_list_sort_short(uint32_t* __restrict__ 
             const unsigned vl = __ballot_sync(FULL, len > kCtaSortMax);
             if (vl && lane == 0) atomicAdd(nlong + 1, (uint32_t)__popc(vl));
         }
-        unsigned mine = __ballot_sync(FULL, len > 1u && len <= kWarpSortMax);
+        unsigned mine = __ballot_sync(FULL, len > min_len && len > 1u && len <= kWarpSortMax);
         while (mine) {
             const int j = __ffs(mine) - 1;
             mine &= mine - 1u;
@@ -217,16 +219,17 @@ __device__ __forceinline__ void cta_bitonic(uint32_t* __restrict__ list, uint32_
 
 // A CTA per list of kWarpSortMax+1 .. kCtaSortMax entries (longer lists are
 // left to k_list_sort_block).
+template <typename OffT>
 __global__ void __launch_bounds__(kCtaSortThreads) k_list_sort_cta(uint32_t* __restrict__ table,
-                                                                   const uint64_t* __restrict__ offsets,
+                                                                   const OffT* __restrict__ offsets,
                                                                    const uint32_t* __restrict__ long_lists,
                                                                    uint32_t nlong) {
     __shared__ uint32_t sb[2][kCtaSortMax];
     int buf = 0;
     for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x) {
         const uint32_t l = long_lists[li];
-        const uint64_t b = offsets[l];
-        const uint32_t n = (uint32_t)(offsets[l + 1] - b);
+        const uint64_t b = (uint64_t)offsets[l];
+        const uint32_t n = (uint32_t)((uint64_t)offsets[l + 1] - b);
         if (n > kCtaSortMax) continue;
         if (n <= 512u) cta_bitonic<2>(table + b, n, sb, buf);
         else if (n <= 1024u) cta_bitonic<4>(table + b, n, sb, buf);
@@ -241,9 +244,10 @@ __global__ void __launch_bounds__(kCtaSortThreads) k_list_sort_cta(uint32_t* __r
 // in the table.  Each pass: a digit histogram of the whole list, then its
 // tiles in order, each ranked stably (per-warp match_any groups in index
 // order) and written at the running offset of its digit.
+template <typename OffT>
 __global__ void __launch_bounds__(kBlockSortThreads) k_list_sort_block(uint32_t* __restrict__ table,
                                                                        uint32_t* __restrict__ scratch,
-                                                                       const uint64_t* __restrict__ offsets,
+                                                                       const OffT* __restrict__ offsets,
                                                                        const uint32_t* __restrict__ long_lists,
                                                                        uint32_t nlong, int passes) {
     __shared__ uint32_t hist[256];
@@ -253,8 +257,8 @@ __global__ void __launch_bounds__(kBlockSortThreads) k_list_sort_block(uint32_t*
     const unsigned lt = lanemask_lt_p();
     for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x) {
         const uint32_t l = long_lists[li];
-        const uint64_t b = offsets[l];
-        const uint32_t n = (uint32_t)(offsets[l + 1] - b);
+        const uint64_t b = (uint64_t)offsets[l];
+        const uint32_t n = (uint32_t)((uint64_t)offsets[l + 1] - b);
         if (n <= kCtaSortMax) continue;  // block-uniform: sorted by k_list_sort_cta
         uint32_t* src = table + b;
         uint32_t* dst = scratch + b;
@@ -316,7 +320,8 @@ size_t place_temp_bytes(uint64_t nlists) {
     return (nlists + 64) * sizeof(uint32_t) + scan_u32_u64_temp_bytes(nlists) + 256;
 }
 
-cudaError_t sort_short_lists(uint32_t* table, const uint64_t* offsets, uint32_t nlists, void* temp,
+template <typename OffT>
+cudaError_t sort_short_lists(uint32_t* table, const OffT* offsets, uint32_t nlists, uint32_t min_len, void* temp,
                              uint32_t* d_nlong, uint32_t* h_nlong, uint32_t* h_nvery, int num_sms, int* launches,
                              cudaStream_t st) {
     *h_nlong = *h_nvery = 0;
@@ -324,7 +329,7 @@ cudaError_t sort_short_lists(uint32_t* table, const uint64_t* offsets, uint32_t 
     cudaError_t e = cudaMemsetAsync(d_nlong, 0, 2 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const unsigned g = grid_for((uint64_t)nlists, 256, (uint64_t)num_sms * 64);
-    k_list_sort_short<<<g, 256, 0, st>>>(table, offsets, nlists, static_cast<uint32_t*>(temp), d_nlong);
+    k_list_sort_short<OffT><<<g, 256, 0, st>>>(table, offsets, nlists, min_len, static_cast<uint32_t*>(temp), d_nlong);
     if (launches) *launches += 1;
     uint32_t h[2];
     e = cudaMemcpyAsync(h, d_nlong, sizeof(h), cudaMemcpyDeviceToHost, st);
@@ -335,13 +340,14 @@ cudaError_t sort_short_lists(uint32_t* table, const uint64_t* offsets, uint32_t 
     return e;
 }
 
-cudaError_t sort_long_lists(uint32_t* table, uint32_t* scratch, const uint64_t* offsets, const void* temp,
+template <typename OffT>
+cudaError_t sort_long_lists(uint32_t* table, uint32_t* scratch, const OffT* offsets, const void* temp,
                             uint32_t nlong, uint32_t nvery, uint32_t id_bits, int num_sms, int* launches,
                             cudaStream_t st) {
     if (nlong == 0) return cudaSuccess;
     const uint32_t* ll = static_cast<const uint32_t*>(temp);
     if (nlong > nvery) {
-        k_list_sort_cta<<<grid_for(nlong - nvery, 1, (uint64_t)num_sms * 6), kCtaSortThreads, 0, st>>>(
+        k_list_sort_cta<OffT><<<grid_for(nlong - nvery, 1, (uint64_t)num_sms * 6), kCtaSortThreads, 0, st>>>(
             table, offsets, ll, nlong);
         if (launches) *launches += 1;
     }
@@ -349,12 +355,21 @@ cudaError_t sort_long_lists(uint32_t* table, uint32_t* scratch, const uint64_t* 
         if (!scratch) return cudaErrorInvalidValue;
         int passes = (int)((id_bits + 7u) / 8u);
         passes += passes & 1;  // even: the sorted list ends in the table
-        k_list_sort_block<<<grid_for(nvery, 1, (uint64_t)num_sms * 8), kBlockSortThreads, 0, st>>>(
+        k_list_sort_block<OffT><<<grid_for(nvery, 1, (uint64_t)num_sms * 8), kBlockSortThreads, 0, st>>>(
             table, scratch, offsets, ll, nlong, passes);
         if (launches) *launches += 1;
     }
     return cudaGetLastError();
 }
+
+template cudaError_t sort_short_lists<uint64_t>(uint32_t*, const uint64_t*, uint32_t, uint32_t, void*, uint32_t*,
+                                                uint32_t*, uint32_t*, int, int*, cudaStream_t);
+template cudaError_t sort_short_lists<uint32_t>(uint32_t*, const uint32_t*, uint32_t, uint32_t, void*, uint32_t*,
+                                                uint32_t*, uint32_t*, int, int*, cudaStream_t);
+template cudaError_t sort_long_lists<uint64_t>(uint32_t*, uint32_t*, const uint64_t*, const void*, uint32_t,
+                                               uint32_t, uint32_t, int, int*, cudaStream_t);
+template cudaError_t sort_long_lists<uint32_t>(uint32_t*, uint32_t*, const uint32_t*, const void*, uint32_t,
+                                               uint32_t, uint32_t, int, int*, cudaStream_t);
 
 cudaError_t place_pairs(const unsigned long long* keys, uint64_t nkeys, uint32_t shift, uint32_t nlists,
                         uint32_t* counts, uint64_t* offsets, uint32_t* table, uint64_t cap, uint32_t* cursor,

@@ -342,3 +342,21 @@ def test_large_properties():
     assert np.array_equal(fwd, rev)  # (q,c) present iff (c,q) present
     # the count pass may use either traversal on low-dimensional grids
     assert s1["candidates"] <= s0["candidates"]
+
+
+@pytest.mark.parametrize("dims,k", [(2, 2), (5, 5)])
+def test_extent_rounding_is_rejected(dims, k):
+    """eps below the float resolution of the data: max + eps rounds to max, so
+    the largest coordinate's cell index equals the grid's extent (the
+    reference would index past its grid).  The join fails with a status, on
+    the dense (2-D, counting sort) and the sparse (5-D, 2^30 cells: radix sort
+    and hash table) grids."""
+    from gpu_self_join_b200._native import GsjError
+
+    rng = np.random.default_rng(5)
+    pts = (1e8 - 8.0 * rng.integers(0, 9, size=(2000, dims))).astype(np.float32)
+    with pytest.raises(GsjError, match="extent"):
+        run_gpu(pts, 1.0, indexed_dims=k)
+    # a representable eps on the same data joins normally
+    c, t, st = run_gpu(pts, 16.0, indexed_dims=k)
+    assert st["total_pairs"] == t.size > 0
