@@ -474,7 +474,18 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 const uint32_t f = t * kSC + pt;
                 uint32_t slot = kNone;
                 if (f < total) {
-                    while (nb_pref[e + 1] <= f) e++;
+                    // the neighbour range holding f: nb_pref[e] <= f < nb_pref[e + 1]
+                    // (f grows by kSC per tile; small cells make a linear walk long,
+                    // so the range is found by bisection unless it is the next one)
+                    if (nb_pref[e + 1] <= f) {
+                        uint32_t lo = e + 1, hi = nnb;  // nb_pref[lo] <= f < nb_pref[hi]
+                        while (hi - lo > 1u) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            if (nb_pref[mid] <= f) lo = mid;
+                            else hi = mid;
+                        }
+                        e = lo;
+                    }
                     slot = nb_start[e] + (f - nb_pref[e]);
                 }
                 c_slot[b * kSC + pt] = slot;
@@ -567,14 +578,18 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 for (uint32_t c32 = colbase; c32 < col_end; c32 += 32u) {
                   float d32[32];
                   tmem_ld32(tmem + s * kTmemCols + ((quarter * 32u) << 16) + c32, d32);
-                  // the columns not provably above G (NaN counts as undecided), one
-                  // comparison per pair; the common case is none in the whole warp
+                  // common case: every value of the 32 columns above G (NaN counts as
+                  // undecided), one predicated comparison per pair
+                  bool all_out = true;
+#pragma unroll
+                  for (int jj = 0; jj < 32; jj++) all_out = all_out && (d32[jj] > G);
+                  if (__all_sync(FULL, !qvalid || all_out || c32 >= nvalid)) continue;
+                  // the undecided columns of this warp's rows
                   unsigned und32 = 0u;
 #pragma unroll
                   for (int jj = 0; jj < 32; jj++) und32 |= (d32[jj] > G) ? 0u : (1u << jj);
                   if (!qvalid) und32 = 0u;
                   if (c32 + 32u > nvalid) und32 &= (c32 >= nvalid) ? 0u : ((1u << (nvalid - c32)) - 1u);
-                  if (!__any_sync(FULL, und32 != 0u)) continue;
                   // appended in two halves of 16 columns (at most 512 entries per
                   // warp and step, the chunk bound of the retry capacity)
                   for (uint32_t h16 = 0; h16 < 2u; h16++) {
