@@ -1013,12 +1013,11 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     GSJ_TRY(dev_get(c, c->minarr, k, &d_min));
     GSJ_CUDA(c, cudaMemcpyAsync(d_min, minArr.data(), k * sizeof(T), cudaMemcpyHostToDevice, st));
 
-    // ---- points ordered by cell, ties by point id (subsystem (a)).  Dense grids
-    // (a slot-prefix table over every linear cell id): a counting sort - cell
-    // ids with per-cell counts and arrival ranks, the scan of the counts (which
-    // is the slot-prefix table), a scatter, then the ids of every cell sorted
-    // ascending.  Other grids: a stable LSD radix sort of keys generated in
-    // point-id order.
+    // ---- cell keys + radix sort (subsystem (a)): points ordered by cell, ties
+    // by point id (a stable sort of keys generated in point-id order).  (A
+    // counting sort through the dense slot table was measured slower on the 2-D
+    // workload: its scatter of ids to random slots took 1.2 ms at 20M points,
+    // more than the four coalesced radix passes.)
     uint64_t *keys = nullptr, *keys2 = nullptr;
     uint32_t *vals = nullptr, *ids = nullptr;
     GSJ_TRY(dev_get(c, c->keys, N, &keys));
@@ -1028,32 +1027,16 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     int bits = 1;
     while (bits < 64 && (totalCells - 1) >> bits) bits++;
     const bool key32 = bits <= 32;
-    const uint64_t dense_limit = std::max<uint64_t>(1u << 24, 8ull * N);
-    const bool dense = totalCells <= dense_limit && totalCells < (1ull << 30);
     void* temp = nullptr;
-    GSJ_TRY(dev_get(c, c->temp,
-                    std::max({radix_sort_temp_bytes(N), runs_temp_bytes(N),
-                              dense ? scan_u32_u64_temp_bytes(totalCells) : (size_t)0}),
-                    (unsigned char**)&temp));
+    GSJ_TRY(dev_get(c, c->temp, std::max(radix_sort_temp_bytes(N), runs_temp_bytes(N)), (unsigned char**)&temp));
     bool in_alt = false;
     int nl = 0;
-    uint32_t *ds = nullptr, *dcnt = nullptr;
     // the number of non-empty cells (word 0) and the out-of-range flag of the
     // cell keys (word 1)
     uint32_t* d_nruns = reinterpret_cast<uint32_t*>(d_mm + 2 * kMaxK);
     GSJ_CUDA(c, cudaMemsetAsync(d_nruns, 0, 2 * sizeof(uint32_t), st));
     S.kernel_launches += 1;
-    if (dense) {
-        GSJ_TRY(dev_get(c, c->dense, totalCells + 1, &ds));
-        GSJ_TRY(dev_get(c, c->dcnt, totalCells + 1, &dcnt));
-        GSJ_CUDA(c, cudaMemsetAsync(dcnt, 0, (totalCells + 1) * sizeof(uint32_t), st));
-        uint32_t* k32 = reinterpret_cast<uint32_t*>(keys);
-        GSJ_CUDA(c, launch_cell_keys_count<T>(d_in, N, n, d_perm, g, d_min, eps, k32, dcnt, vals, d_nruns + 1, st));
-        // ds[L] = points in cells below L (ds[totalCells] = N)
-        S.kernel_launches += 4;
-        GSJ_CUDA(c, scan_u32_u32(dcnt, ds, totalCells, temp, st));
-        GSJ_CUDA(c, launch_count_scatter(k32, vals, ds, N, reinterpret_cast<uint32_t*>(keys2), ids, st));
-    } else if (key32) {
+    if (key32) {
         uint32_t* k32 = reinterpret_cast<uint32_t*>(keys);
         uint32_t* k32b = reinterpret_cast<uint32_t*>(keys2);
         GSJ_CUDA(c, (launch_cell_keys<T, uint32_t>(d_in, N, n, d_perm, g, d_min, eps, k32, vals, d_nruns + 1, st)));
@@ -1063,7 +1046,7 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         GSJ_CUDA(c, radix_sort<uint64_t>(keys, keys2, vals, ids, N, 0, bits, temp, &in_alt, &nl, st));
     }
     S.kernel_launches += (uint64_t)nl;
-    if (!dense && !in_alt) {
+    if (!in_alt) {
         // an even number of passes (or none) leaves the result in the first buffers
         std::swap(c->keys, c->keys2);
         std::swap(c->vals, c->ids);
@@ -1089,27 +1072,6 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
                     "a coordinate maps to the grid's extent (epsilon below the resolution of the data's type)");
     const uint32_t M = runs[0];
     S.nonempty_cells = M;
-    if (dense && N > 1) {
-        // counting sort: each cell's ids ascending (small cells one thread each,
-        // larger ones by the list sorts; the rank buffer is free as scratch)
-        constexpr uint32_t kSmallCell = 16;
-        S.kernel_launches += 2;
-        GSJ_CUDA(c, launch_cell_ids_small(ids, cell_start, M, kSmallCell, st));
-        void* ptemp = nullptr;
-        GSJ_TRY(dev_get(c, c->ptemp, place_temp_bytes(M), (unsigned char**)&ptemp));
-        uint32_t* d_nlong = reinterpret_cast<uint32_t*>(c->misc.p) + 4 * kMaxK + 24;
-        uint32_t nlong = 0, nvery = 0;
-        int nls = 0;
-        GSJ_CUDA(c, sort_short_lists<uint32_t>(ids, cell_start, M, kSmallCell, ptemp, d_nlong, &nlong, &nvery,
-                                               c->num_sms, &nls, st));
-        if (nlong) {
-            uint32_t id_bits = 1;
-            while (id_bits < 32 && ((N - 1) >> id_bits)) id_bits++;
-            GSJ_CUDA(c, sort_long_lists<uint32_t>(ids, vals, cell_start, ptemp, nlong, nvery, id_bits, c->num_sms,
-                                                  &nls, st));
-        }
-        S.kernel_launches += (uint64_t)nls;
-    }
 
     // ---- SORT (GPU.cu:351-395): each cell's points ordered by their value in the
     // sort dimension with std::sort and the reference's comparator, on the host
@@ -1152,19 +1114,31 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
     // ---- cell lookup: on dense grids a slot-prefix table over every linear
     // cell id (cell L holds slots [ds[L], ds[L+1])), else a hash table of the
     // non-empty cells
-    // (dense grids: ds was built with the counting sort)
+    uint32_t *ds = nullptr, *dcnt = nullptr;
     unsigned long long* hkeys = nullptr;
     uint32_t* hvals = nullptr;
     uint64_t hmask = 0;
-    if (!dense) {
+    const uint64_t dense_limit = std::max<uint64_t>(1u << 24, 8ull * N);
+    const bool dense = totalCells <= dense_limit && totalCells < (1ull << 30);
+    if (dense) {
+        GSJ_TRY(dev_get(c, c->dense, totalCells + 1, &ds));
+        GSJ_TRY(dev_get(c, c->dcnt, totalCells + 1, &dcnt));
+        GSJ_CUDA(c, cudaMemsetAsync(dcnt, 0, (totalCells + 1) * sizeof(uint32_t), st));
+    } else {
         uint64_t hcap = 1024;
         while (hcap < 2ull * M) hcap <<= 1;
         hmask = hcap - 1;
         GSJ_TRY(dev_get(c, c->hkeys, hcap, &hkeys));
         GSJ_TRY(dev_get(c, c->hvals, hcap, &hvals));
         GSJ_CUDA(c, cudaMemsetAsync(hkeys, 0xff, hcap * sizeof(unsigned long long), st));
-        S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, M, nullptr, hkeys, hvals, hmask, st));
+    }
+    S.kernel_launches += 1;
+    GSJ_CUDA(c, launch_cell_tables(cell_key, cell_start, M, dcnt, hkeys, hvals, hmask, st));
+    if (dense) {
+        // the slot-prefix table: ds[L] = points in cells below L (ds[totalCells] = N)
+        GSJ_TRY(dev_get(c, c->temp, scan_u32_u64_temp_bytes(totalCells), (unsigned char**)&temp));
+        S.kernel_launches += 3;
+        GSJ_CUDA(c, scan_u32_u32(dcnt, ds, totalCells, temp, st));
     }
     // Dense low-dimensional grids use the row-range traversal driven by a
     // per-cell plan of neighbour-row slot ranges.

@@ -164,57 +164,6 @@ __global__ void k_cell_keys(const T* __restrict__ in, uint64_t N, uint32_t n, co
     vals[i] = (uint32_t)i;
 }
 
-// Dense grids: the cell id of every point (the formula of k_cell_keys) and
-// its arrival rank among the points of its cell, rank[i] = dcnt[key] before
-// point i's increment (dcnt zeroed by the caller; afterwards the points per
-// cell id).
-template <typename T>
-__global__ void k_cell_keys_count(const T* __restrict__ in, uint64_t N, uint32_t n, const uint32_t* __restrict__ perm,
-                                  GridGeom g, const T* __restrict__ minArr, T eps, uint32_t* __restrict__ keys,
-                                  uint32_t* __restrict__ dcnt, uint32_t* __restrict__ rank, uint32_t* __restrict__ bad) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    // every index below its extent: key < the product of the extents = the
-    // table size (an out-of-range point is cell 0 and flagged)
-    const uint64_t key = cell_key_of<T>(in, i, n, perm, g, minArr, eps, bad);
-    keys[i] = (uint32_t)key;
-    rank[i] = atomicAdd(&dcnt[key], 1u);
-}
-
-// Counting-sort scatter: point i goes to slot ds[key] + rank (cells in id
-// order; inside a cell in arrival order until k_cell_ids_small and the list
-// sorts order the ids ascending).
-__global__ void k_count_scatter(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ rank,
-                                const uint32_t* __restrict__ ds, uint64_t N, uint32_t* __restrict__ keys_out,
-                                uint32_t* __restrict__ ids_out) {
-    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const uint32_t key = keys[i];
-    const uint32_t p = ds[key] + rank[i];
-    keys_out[p] = key;
-    ids_out[p] = (uint32_t)i;
-}
-
-// The ids of every cell of 2..small points ascending (insertion sort by one
-// thread); larger cells are left to the list sorts.
-__global__ void k_cell_ids_small(uint32_t* __restrict__ ids, const uint32_t* __restrict__ cell_start, uint32_t M,
-                                 uint32_t small) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= M) return;
-    const uint32_t b = cell_start[c], len = cell_start[c + 1] - b;
-    if (len < 2u || len > small) return;
-    uint32_t* a = ids + b;
-    for (uint32_t i = 1; i < len; i++) {
-        const uint32_t x = a[i];
-        uint32_t j = i;
-        while (j > 0 && a[j - 1] > x) {
-            a[j] = a[j - 1];
-            j--;
-        }
-        a[j] = x;
-    }
-}
-
 // Points in cell order with reordered, zero-padded columns: pts[s][j] = in[ids[s]][perm[j]].
 template <typename T>
 __global__ void k_gather_points(const T* __restrict__ in, uint64_t N, uint32_t n, uint32_t npad,
@@ -351,29 +300,6 @@ cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t n
     return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_cell_keys_count(const T* in, uint64_t N, uint32_t n, const uint32_t* perm, const GridGeom& g,
-                                   const T* minArr, T eps, uint32_t* keys, uint32_t* dcnt, uint32_t* rank,
-                                   uint32_t* bad, cudaStream_t st) {
-    if (N == 0) return cudaSuccess;
-    k_cell_keys_count<T><<<blocks_for(N, 256), 256, 0, st>>>(in, N, n, perm, g, minArr, eps, keys, dcnt, rank,
-                                                             bad);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_count_scatter(const uint32_t* keys, const uint32_t* rank, const uint32_t* ds, uint64_t N,
-                                 uint32_t* keys_out, uint32_t* ids_out, cudaStream_t st) {
-    if (N == 0) return cudaSuccess;
-    k_count_scatter<<<blocks_for(N, 256), 256, 0, st>>>(keys, rank, ds, N, keys_out, ids_out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_cell_ids_small(uint32_t* ids, const uint32_t* cell_start, uint32_t M, uint32_t small,
-                                  cudaStream_t st) {
-    if (M == 0) return cudaSuccess;
-    k_cell_ids_small<<<blocks_for(M, 256), 256, 0, st>>>(ids, cell_start, M, small);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_cell_tables(const uint64_t* cell_key, const uint32_t* cell_start, uint32_t M, uint32_t* dcnt,
                                unsigned long long* hkeys, uint32_t* hvals, uint64_t hmask, cudaStream_t st) {
@@ -417,10 +343,7 @@ cudaError_t launch_iota(uint32_t* out, uint32_t M, cudaStream_t st) {
                                                        const GridGeom&, const T*, T, uint32_t*, uint32_t*, \
                                                        uint32_t*, cudaStream_t);                           \
     template cudaError_t launch_gather_points<T>(const T*, uint64_t, uint32_t, uint32_t, const uint32_t*,  \
-                                                 const uint32_t*, T*, cudaStream_t);                       \
-    template cudaError_t launch_cell_keys_count<T>(const T*, uint64_t, uint32_t, const uint32_t*,          \
-                                                   const GridGeom&, const T*, T, uint32_t*, uint32_t*,     \
-                                                   uint32_t*, uint32_t*, cudaStream_t);
+                                                 const uint32_t*, T*, cudaStream_t);
 GSJ_INST_INDEX(float)
 GSJ_INST_INDEX(double)
 

@@ -28,19 +28,6 @@ cudaError_t launch_minmax(const T* in, uint64_t N, uint32_t n, uint32_t k, const
 template <typename T, typename K>
 cudaError_t launch_cell_keys(const T* in, uint64_t N, uint32_t n, const uint32_t* perm, const GridGeom& g,
                              const T* minArr, T eps, K* keys, uint32_t* vals, uint32_t* bad, cudaStream_t st);
-// Dense grids (counting sort): 32-bit cell ids, per-cell counts (dcnt zeroed
-// by the caller) and each point's arrival rank within its cell; *bad as above
-// (such a point is counted in cell 0, so every access stays in the table).
-template <typename T>
-cudaError_t launch_cell_keys_count(const T* in, uint64_t N, uint32_t n, const uint32_t* perm, const GridGeom& g,
-                                   const T* minArr, T eps, uint32_t* keys, uint32_t* dcnt, uint32_t* rank,
-                                   uint32_t* bad, cudaStream_t st);
-// Point i to slot ds[keys[i]] + rank[i]: keys_out (cell ids by slot), ids_out.
-cudaError_t launch_count_scatter(const uint32_t* keys, const uint32_t* rank, const uint32_t* ds, uint64_t N,
-                                 uint32_t* keys_out, uint32_t* ids_out, cudaStream_t st);
-// The ids of every cell of 2..small points sorted ascending in place.
-cudaError_t launch_cell_ids_small(uint32_t* ids, const uint32_t* cell_start, uint32_t M, uint32_t small,
-                                  cudaStream_t st);
 template <typename T>
 cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t npad, const uint32_t* perm,
                                  const uint32_t* ids, T* pts, cudaStream_t st);

@@ -349,8 +349,8 @@ def test_extent_rounding_is_rejected(dims, k):
     """eps below the float resolution of the data: max + eps rounds to max, so
     the largest coordinate's cell index equals the grid's extent (the
     reference would index past its grid).  The join fails with a status, on
-    the dense (2-D, counting sort) and the sparse (5-D, 2^30 cells: radix sort
-    and hash table) grids."""
+    the dense (2-D: slot-prefix table) and the sparse (5-D, 2^30 cells: hash
+    table) grids."""
     from gpu_self_join_b200._native import GsjError
 
     rng = np.random.default_rng(5)
