@@ -119,8 +119,12 @@ __device__ __forceinline__ uint32_t cand_slot(const uint32_t* nb_start, const ui
     return f < total ? nb_start[my] + (f - pf) : 0u;
 }
 
+// 4 CTAs of 8 warps per SM for float data (at most 64 registers a thread; the
+// 6-D register path spills 36 bytes): on the 6-D mixture the emit stage went
+// from 38.7 to 34.7 ms against 3 CTAs at 80 registers, the candidate-row loads
+// being latency-bound.
 template <typename T, int NT, int MODEL, int POL, bool STAMP, bool ROWS>
-__global__ void __launch_bounds__(256) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_join(const JoinArgs<T> a, uint32_t nb_cap, uint32_t noff,
                                               const TileOut o, uint32_t nvisit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool GENERIC = (NT == 0);

@@ -33,16 +33,14 @@
 // only make the test inconclusive, which sends the pair to the exact check.
 //
 // Synchronisation: warps 8-11 produce candidate tiles (slot search, cp.async of
-// the rows and norms) and issue the MMA, warps 0-7 consume; candidate tiles
-// rotate through 3 to 6 buffers (as many as fit two CTAs per SM; all but two
-// are copied ahead of the tile whose MMA is issued) and two accumulators
-// alternate, handed over by mbarriers (full: MMA commit + the issuer's
-// release; empty: the consumer arrivals; free: a tile buffer read).  Every
-// wait is a bounded poll by one thread whose verdict is shared before any
-// barrier or warp-collective; on time-out the error flag is raised and the CTA
-// stops.  Tensor memory (2 x 128 columns) is allocated once per CTA; the
-// shared-memory request keeps at most 2 CTAs (512 columns) on an SM; it is
-// released before exit.
+// the rows) and issue the MMA, warps 0-7 consume; candidate tiles rotate
+// through kStages buffers and two accumulators alternate, handed over by
+// mbarriers (full: MMA commit + the issuer's release; empty: the consumer
+// arrivals).  Every wait is a bounded poll by one thread whose verdict is
+// shared before any barrier or warp-collective; on time-out the error flag is
+// raised and the CTA stops.  Tensor memory (2 x 128 columns) is allocated once
+// per CTA; the shared-memory request keeps at most 2 CTAs (512 columns) on an
+// SM; it is released before exit.
 #include <algorithm>
 #include <cstdint>
 #include <cuda_bf16.h>
@@ -65,9 +63,7 @@ constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kMinSmem = 80u * 1024u;  // at most 2 CTAs (2 x 256 TMEM columns) per SM
 constexpr uint32_t kWaitPolls = 1u << 20;
 constexpr uint32_t kBlk = (uint32_t)kScreenBlockSlack;  // undecided-pair entries a consumer warp reserves
-constexpr uint32_t kMinStages = 3;  // candidate tile buffers (the accumulators alternate in 2) ...
-constexpr uint32_t kMaxStages = 6;  // ... as many as fit 2 CTAs per SM; tiles copied ahead: stages - 2
-constexpr uint32_t kScreenSmemCap = 110u * 1024u;  // per CTA, with 2 CTAs per SM
+constexpr uint32_t kStages = 3;     // candidate tiles in flight (the accumulators alternate in 2)
 
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bit 4),
 // A and B BF16 (bits 7 and 10), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
@@ -220,34 +216,32 @@ __device__ float exact_sqdist4(const float* __restrict__ q, const float* __restr
 }
 
 struct ScreenSmem {
-    uint32_t a, b, nbs, nbp, cslot, cnorm, cwmax, qid, qinfo, misc, total;
+    uint32_t a, b, nbs, nbp, cslot, cwmax, qid, qinfo, misc, total;
 };
 
-__host__ __device__ inline ScreenSmem screen_smem(uint32_t kpad, uint32_t noff, uint32_t ns) {
+__host__ __device__ inline ScreenSmem screen_smem(uint32_t kpad, uint32_t noff) {
     ScreenSmem t{};
     uint32_t o = 0;
     t.a = o;
     o += (uint32_t)kSQ * kpad * 2u;
-    t.b = o;  // ns candidate tiles
-    o += ns * (uint32_t)kSC * kpad * 2u;
+    t.b = o;  // kStages candidate tiles
+    o += kStages * (uint32_t)kSC * kpad * 2u;
     t.nbs = o;
     o += noff * 4u;
     t.nbp = o;
     o += (noff + 1u) * 4u;
     o = (o + 15u) & ~15u;
-    t.cslot = o;  // [ns][kSC]
-    o += ns * kSC * 4u;
-    t.cnorm = o;  // [ns][kSC] candidate norms (FP32, copied with the rows)
-    o += ns * kSC * 4u;
-    t.cwmax = o;  // [ns][4] largest candidate norm per producer warp
-    o += ns * 4u * 4u;
+    t.cslot = o;  // [kStages][kSC]
+    o += kStages * kSC * 4u;
+    t.cwmax = o;  // [kStages][4] largest candidate norm per producer warp
+    o += kStages * 4u * 4u;
     t.qid = o;
     o += kSQ * 4u;
     o = (o + 15u) & ~15u;
     t.qinfo = o;  // float4 per query: |q^|^2, R0 + kE |q^|, c1 |q^|^2, valid
     o += kSQ * 16u;
     t.misc = o;   // [0] item [1] failed [2] total [4] tmem [8..19] warp counts
-                  // [24..31] mbarriers full0 full1 empty0 empty1, [32..47] free[0..ns)
+                  // [24..31] mbarriers full0 full1 empty0 empty1, [32..37] free0 free1 free2
     o += 48u * 4u;
     t.total = (o + 127u) & ~127u;
     return t;
@@ -255,21 +249,6 @@ __host__ __device__ inline ScreenSmem screen_smem(uint32_t kpad, uint32_t noff, 
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-}
-
-// Waits until at most n of this thread's committed copy groups are pending.
-__device__ __forceinline__ void cp_async_wait(uint32_t n) {
-    switch (n) {
-        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
-        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
-        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
-        case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
-        default: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
-    }
 }
 
 __device__ __forceinline__ void bar_arrive(uint32_t bar) {
@@ -298,25 +277,22 @@ __device__ __forceinline__ bool named_sync_or(uint32_t id, uint32_t count, bool 
 // The CTA is warp-specialised: warps 8-11 produce (candidate slots, centred
 // BF16 candidate rows with the norm folded in, the MMA), warps 0-7 consume
 // (tensor-memory rows, the screen, the undecided-pair appends).  Candidate
-// tiles rotate through ns buffers and two accumulators alternate; mbarriers
-// full[s] (MMA done), empty[s] (accumulator read) and free[b] (tile buffer
-// read) hand them over.
+// tiles rotate through kStages buffers and two accumulators alternate;
+// mbarriers full[s] (MMA done) and empty[s] (accumulator read) hand them over.
 //
 // With the norm folded into the product (A row, the query = [-2 q^, 1, 1];
 // B row, the candidate = [c^, |c^|^2_hi, |c^|^2_lo]), the accumulator holds
 // |c^_j|^2 - 2 q^_i.c^_j directly and the screen is one comparison per pair.
 template <int MODEL, bool STAMP>
 __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<float> a, const TileOut o,
-                                                              const ScreenConst sc, uint32_t noff, uint32_t nvisit,
-                                                              uint32_t ns) {
+                                                              const ScreenConst sc, uint32_t noff, uint32_t nvisit) {
     extern __shared__ __align__(1024) unsigned char ssm[];
     const uint32_t n = a.n, npad = a.npad, k = a.g.k, kpad = sc.kpad;
-    const ScreenSmem L = screen_smem(kpad, noff, ns);
+    const ScreenSmem L = screen_smem(kpad, noff);
     unsigned char* A = ssm + L.a;
     uint32_t* nb_start = reinterpret_cast<uint32_t*>(ssm + L.nbs);
     uint32_t* nb_pref = reinterpret_cast<uint32_t*>(ssm + L.nbp);
     uint32_t* c_slot = reinterpret_cast<uint32_t*>(ssm + L.cslot);
-    float* cnorm = reinterpret_cast<float*>(ssm + L.cnorm);
     float* cwmax = reinterpret_cast<float*>(ssm + L.cwmax);
     uint32_t* q_id = reinterpret_cast<uint32_t*>(ssm + L.qid);
     float4* qinfo = reinterpret_cast<float4*>(ssm + L.qinfo);
@@ -339,7 +315,7 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(empty0) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(empty1) : "memory");
         // free[b]: the consumers are done with stage b (candidate tile, slots, norm bound)
-        for (uint32_t b = 0; b < ns; b++)
+        for (uint32_t b = 0; b < kStages; b++)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(free0 + 8u * b) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -458,40 +434,27 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
         cand_total += (unsigned long long)total * qn;
 
         if (tid >= kProd0) {
-            // ================= producer warps: tiles t + 1 .. t + ns - 2 copied ahead
-            // (slots, cp.async of the rows and norms) when tile t is completed
-            // (copies landed, the tile's norm bound, MMA issued)
+            // ================= producer warps: stage tile t + 1 (slots, cp.async of
+            // the rows) before completing tile t (copies landed, MMA issued)
             const uint32_t pt = (uint32_t)tid - (uint32_t)kProd0;  // candidate row of the tile
-            const uint32_t la = ns - 2u;
             // the copy walks (row, chunk) pairs in row-major order, 128 apart
             const uint32_t step_r = (uint32_t)kSC / kch, step_c = (uint32_t)kSC % kch;
             uint32_t e = 0;  // neighbour range of this thread's current candidate (f grows by kSC per tile)
             auto prepare = [&](uint32_t t) -> bool {
-                const uint32_t g = tiles_done + t, b = g % ns;
+                const uint32_t g = tiles_done + t, b = g % kStages;
                 bool bad = false;
-                if (g >= ns && pt == 0) bad = !bar_wait_bounded(free0 + 8u * b, ((g / ns) - 1u) & 1u);
+                if (g >= kStages && pt == 0) bad = !bar_wait_bounded(free0 + 8u * b, ((g / kStages) - 1u) & 1u);
                 if (named_sync_or(1, 128, bad)) return false;
                 const uint32_t f = t * kSC + pt;
                 uint32_t slot = kNone;
+                float wm = 0.f;
                 if (f < total) {
-                    // the neighbour range holding f: nb_pref[e] <= f < nb_pref[e + 1]
-                    // (f grows by kSC per tile; small cells make a linear walk long,
-                    // so the range is found by bisection unless it is the next one)
-                    if (nb_pref[e + 1] <= f) {
-                        uint32_t lo = e + 1, hi = nnb;  // nb_pref[lo] <= f < nb_pref[hi]
-                        while (hi - lo > 1u) {
-                            const uint32_t mid = (lo + hi) >> 1;
-                            if (nb_pref[mid] <= f) lo = mid;
-                            else hi = mid;
-                        }
-                        e = lo;
-                    }
+                    while (nb_pref[e + 1] <= f) e++;
                     slot = nb_start[e] + (f - nb_pref[e]);
+                    // |c^|^2 in FP32 bounds the folded hi + lo terms
+                    wm = sc.norms[slot];
                 }
                 c_slot[b * kSC + pt] = slot;
-                // |c^|^2 in FP32 bounds the folded hi + lo terms (0 for an empty column)
-                cp_async4(smem_u32(cnorm + b * kSC + pt), sc.norms + (slot != kNone ? slot : 0u),
-                          slot != kNone ? 4u : 0u);
                 named_sync(1, 128);
                 {
                     const uint32_t dst = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
@@ -510,15 +473,15 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                     }
                     asm volatile("cp.async.commit_group;" ::: "memory");
                 }
-                return true;
-            };
-            auto complete = [&](uint32_t t, uint32_t pending) -> bool {
-                const uint32_t g = tiles_done + t, b = g % ns, s = g & 1u;
-                cp_async_wait(pending);
-                float wm = cnorm[b * kSC + pt];  // this thread's own copy, landed
 #pragma unroll
                 for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
                 if (lane == 0) cwmax[b * 4u + (uint32_t)(warp - 8)] = wm;
+                return true;
+            };
+            auto complete = [&](uint32_t t, bool next_pending) -> bool {
+                const uint32_t g = tiles_done + t, b = g % kStages, s = g & 1u;
+                if (next_pending) asm volatile("cp.async.wait_group 1;" ::: "memory");
+                else asm volatile("cp.async.wait_group 0;" ::: "memory");
                 fence_async_smem();
                 bool bad = false;
                 if (g >= 2 && pt == 0) bad = !bar_wait_bounded((s ? empty1 : empty0), ((g >> 1) - 1u) & 1u);
@@ -539,12 +502,10 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 }
                 return true;
             };
-            bool ok = true;
-            for (uint32_t t = 0; ok && t < la && t < T; t++) ok = prepare(t);
+            bool ok = T == 0 || prepare(0);
             for (uint32_t t = 0; ok && t < T; t++) {
-                if (t + la < T) ok = prepare(t + la);
-                // copy groups committed after tile t's: tiles t + 1 .. min(t + la, T - 1)
-                if (ok) ok = complete(t, min(la, T - 1u - t));
+                if (t + 1 < T) ok = prepare(t + 1);
+                if (ok) ok = complete(t, t + 1 < T);
             }
             asm volatile("cp.async.wait_all;" ::: "memory");
             if (!ok && pt == 0) misc[1] = 1u;
@@ -565,7 +526,7 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                     break;
                 }
                 fence_after();
-                const uint32_t b = g % ns;
+                const uint32_t b = g % kStages;
                 const float cmax = cwmax[b * 4u], rcmax = cwmax[b * 4u + 1u];
                 // G_i from the tile's largest candidate norm (an upper bound of every column's bound)
                 const float tt = __fmaf_ru(sc.ke, rcmax, qi.y);
@@ -578,23 +539,19 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 for (uint32_t c32 = colbase; c32 < col_end; c32 += 32u) {
                   float d32[32];
                   tmem_ld32(tmem + s * kTmemCols + ((quarter * 32u) << 16) + c32, d32);
-                  // common case: every value of the 32 columns above G (NaN counts as
-                  // undecided), one predicated comparison per pair
+                  // common case: every value of the 32 columns above G (NaN counts as undecided)
                   bool all_out = true;
 #pragma unroll
                   for (int jj = 0; jj < 32; jj++) all_out = all_out && (d32[jj] > G);
                   if (__all_sync(FULL, !qvalid || all_out || c32 >= nvalid)) continue;
-                  // the undecided columns of this warp's rows
-                  unsigned und32 = 0u;
-#pragma unroll
-                  for (int jj = 0; jj < 32; jj++) und32 |= (d32[jj] > G) ? 0u : (1u << jj);
-                  if (!qvalid) und32 = 0u;
-                  if (c32 + 32u > nvalid) und32 &= (c32 >= nvalid) ? 0u : ((1u << (nvalid - c32)) - 1u);
-                  // appended in two halves of 16 columns (at most 512 entries per
-                  // warp and step, the chunk bound of the retry capacity)
                   for (uint32_t h16 = 0; h16 < 2u; h16++) {
                     const uint32_t col0 = c32 + 16u * h16;
-                    const unsigned und = (und32 >> (16u * h16)) & 0xffffu;
+                    unsigned und = 0;
+                    if (qvalid) {
+#pragma unroll
+                        for (int jj = 0; jj < 16; jj++) und |= (d32[16 * h16 + jj] > G) ? 0u : (1u << jj);
+                        if (col0 + 16u > nvalid) und &= (col0 >= nvalid) ? 0u : ((1u << (nvalid - col0)) - 1u);
+                    }
                     if (!__any_sync(FULL, und != 0u)) continue;
                     // the undecided pairs (query slot | cross << 31, candidate slot) go to
                     // the exact check (k_screen_recheck), one atomic per warp and chunk
@@ -662,10 +619,7 @@ template <int MODEL, bool STAMP>
 cudaError_t launch_screen_one(const JoinArgs<float>& a, const TileOut& o, const ScreenConst& sc, uint32_t noff,
                               uint32_t nvisit, int num_sms, cudaStream_t st) {
     auto kern = k_tile_screen<MODEL, STAMP>;
-    // as many tile buffers as fit the per-CTA share of 2 CTAs per SM
-    uint32_t ns = kMaxStages;
-    while (ns > kMinStages && screen_smem(sc.kpad, noff, ns).total > kScreenSmemCap) ns--;
-    const ScreenSmem L = screen_smem(sc.kpad, noff, ns);
+    const ScreenSmem L = screen_smem(sc.kpad, noff);
     const uint32_t smem = L.total > kMinSmem ? L.total : kMinSmem;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -682,7 +636,7 @@ cudaError_t launch_screen_one(const JoinArgs<float>& a, const TileOut& o, const 
     if (a.shape_per_sm && (int)a.shape_per_sm < per_sm) per_sm = (int)a.shape_per_sm;
     uint64_t blocks = (uint64_t)num_sms * per_sm;
     if (blocks > nvisit) blocks = nvisit ? nvisit : 1;
-    kern<<<(unsigned)blocks, kSThreads, smem, st>>>(a, o, sc, noff, nvisit, ns);
+    kern<<<(unsigned)blocks, kSThreads, smem, st>>>(a, o, sc, noff, nvisit);
     return cudaGetLastError();
 }
 
