@@ -440,6 +440,7 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
             // the copy walks (row, chunk) pairs in row-major order, 128 apart
             const uint32_t step_r = (uint32_t)kSC / kch, step_c = (uint32_t)kSC % kch;
             uint32_t e = 0;  // neighbour range of this thread's current candidate (f grows by kSC per tile)
+            float wm_cur = 0.f, wm_next = 0.f;  // candidate norms of the last two prepared tiles
             auto prepare = [&](uint32_t t) -> bool {
                 const uint32_t g = tiles_done + t, b = g % kStages;
                 bool bad = false;
@@ -447,17 +448,27 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 if (named_sync_or(1, 128, bad)) return false;
                 const uint32_t f = t * kSC + pt;
                 uint32_t slot = kNone;
-                float wm = 0.f;
+                wm_cur = wm_next;
+                wm_next = 0.f;
                 if (f < total) {
                     while (nb_pref[e + 1] <= f) e++;
                     slot = nb_start[e] + (f - nb_pref[e]);
-                    // |c^|^2 in FP32 bounds the folded hi + lo terms
-                    wm = sc.norms[slot];
+                    // |c^|^2 in FP32 bounds the folded hi + lo terms (reduced when the
+                    // tile is completed, so that the load's latency is not waited for here)
+                    wm_next = sc.norms[slot];
                 }
                 c_slot[b * kSC + pt] = slot;
-                named_sync(1, 128);
-                {
-                    const uint32_t dst = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
+                const uint32_t dst = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
+                if (kch <= 4u) {
+                    // short rows (up to 32 values): each thread copies its own row, no barrier
+                    const bool valid = slot != kNone;
+                    const uint4* src = sc.rows + (size_t)(valid ? slot : 0u) * kch;
+                    for (uint32_t kc = 0; kc < kch; kc++)
+                        cp_async16(dst + core_off(pt, kc, kpad), src + kc, valid ? 16u : 0u);
+                    asm volatile("cp.async.commit_group;" ::: "memory");
+                } else {
+                    // longer rows: consecutive threads copy consecutive chunks of a row
+                    named_sync(1, 128);
                     uint32_t r = pt / kch, kc = pt % kch;
                     for (uint32_t j = 0; j < kch; j++) {
                         const uint32_t sl = c_slot[b * kSC + r];
@@ -473,13 +484,15 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                     }
                     asm volatile("cp.async.commit_group;" ::: "memory");
                 }
-#pragma unroll
-                for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
-                if (lane == 0) cwmax[b * 4u + (uint32_t)(warp - 8)] = wm;
                 return true;
             };
             auto complete = [&](uint32_t t, bool next_pending) -> bool {
                 const uint32_t g = tiles_done + t, b = g % kStages, s = g & 1u;
+                // tile t's norms: loaded by prepare(t), i.e. wm_cur once prepare(t + 1) ran
+                float wm = next_pending ? wm_cur : wm_next;
+#pragma unroll
+                for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
+                if (lane == 0) cwmax[b * 4u + (uint32_t)(warp - 8)] = wm;
                 if (next_pending) asm volatile("cp.async.wait_group 1;" ::: "memory");
                 else asm volatile("cp.async.wait_group 0;" ::: "memory");
                 fence_async_smem();

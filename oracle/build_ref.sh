@@ -13,7 +13,8 @@
 # builds, which report the same pair set.
 #
 # The binaries are test infrastructure: the oracle's pin against the reference
-# (tests/golden/make_ref_fixtures.py) and the reference arm of bench.py.
+# (tests/golden/make_ref_fixtures.py), the reference arm of bench.py, and the
+# reference's own timing of the benchmarked workloads (tests/golden/time_ref_gpu.py).
 #
 # usage: oracle/build_ref.sh [REFERENCE_DIR]
 #   (default: $GSJ_REFERENCE_DIR, else the checkout at /root/reference)
@@ -45,6 +46,11 @@ CONFIGS=(
   "d2_sort           2 2 float  0 0 0 0 0 1 1"
   "d3_k2_sort        3 2 float  0 0 0 0 0 1 1"
   "d5_k3_f64_sort    5 3 double 0 1 2 1 0 1 1"
+  # timing builds of the benchmarked workloads (no neighbour-table print)
+  "t_d2   2 2 float 0 0 0 0 0 0"
+  "t_d6   6 6 float 0 0 0 0 0 0"
+  "t_d18 18 6 float 0 1 8 1 1 0"
+  "t_d90 90 6 float 0 1 8 1 1 0"
 )
 
 write_params() {  # $1 dir, then the fields
