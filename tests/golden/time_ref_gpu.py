@@ -48,7 +48,7 @@ def main() -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", default="")
-    ap.add_argument("--out", default=os.path.join(ROOT, "ref_gpu_times.json"))
+    ap.add_argument("--out", default=os.path.join(HERE, "ref_gpu_times.json"))
     a = ap.parse_args()
     names = [x for x in BUILD_OF if not a.only or x in a.only.split(",")]
     res = {}
