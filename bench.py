@@ -537,7 +537,9 @@ def _ours(args) -> None:
         d2h = int(4 * N + 4 * R)
         e2e = {"value": pairs_all / (ems / 1e3), "unit": "pairs/s", "ms_per_step": ems / args.steps,
                "h2d_bytes_per_step": int(N * n * 4), "d2h_bytes_per_step": d2h,
-               "batches": int(est[-1]["batches"]), "api": "gsj_join_host (pinned host buffers)"}
+               "batches": int(est[-1]["batches"]), "api": "gsj_join_host (pinned host buffers)",
+               "host_ms": {k: float(np.mean([e[k] for e in est]))
+                           for k in ("ms_h2d", "ms_index", "ms_join", "ms_d2h", "ms_total")}}
         link = _link_peaks(max(d2h, 1 << 26))
         if link:
             t_link = (N * n * 4) / (link["h2d_gbs"] * 1e9) + d2h / (link["d2h_gbs"] * 1e9)
