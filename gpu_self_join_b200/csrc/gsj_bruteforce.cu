@@ -6,7 +6,7 @@
 // sequential model of gsj_dist.cuh with the pinned contraction policy) and
 // `sqrt(runningDist) <= eps` as `s <= thr`.  The reference accumulates one
 // global total; here each point's count is written as well, which makes the
-// kernel an exact-count judge for the grid join on small inputs.
+// kernel an exact-count check of the grid join on small inputs.
 //
 // Layout: a CTA of 256 queries walks all points in tiles of kBfTile rows
 // staged in shared memory; every thread keeps its own count (no atomics but

@@ -220,7 +220,7 @@ GSJ_API double gsj_threshold_f64(double eps);
  * (`runningDist += (c-q)*(c-q)` over the dimensions in order, sqrt <= eps).
  * cfg supplies dim and dtype (the index switches do not apply).  counts
  * (optional, host, uint32[N]) receives each point's count, total the sum.
- * O(N^2 n) work: an exact-count judge for the grid join on small inputs. */
+ * O(N^2 n) work: an exact-count check of the grid join on small inputs. */
 GSJ_API int gsj_bruteforce_count(gsj_context* ctx, const void* data, uint64_t num_points, double eps,
                                  const gsj_config* cfg, int data_on_device, uint32_t* counts,
                                  uint64_t* total);
@@ -286,7 +286,7 @@ GSJ_API int gsj_tuning_set(gsj_context* ctx, uint32_t path, uint32_t dim, uint32
  * cell's queries from the sizes of the cell and its face-adjacent cells, eps
  * and the dimensionality.  It replaces the reference's sampled estimator
  * (callGPUBatchEst, GPU.cu:57-268; SAMPLERATE, params.h:93) for sizing the
- * pair buffers; the exact count still judges every buffer.  Training and
+ * pair buffers; the exact count still checks every buffer.  Training and
  * inference run on the device with this library's own kernels. */
 #define GSJ_MODEL_WEIGHTS 3201
 #define GSJ_MODEL_FEATURES 16
