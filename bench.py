@@ -32,6 +32,7 @@ import json
 import os
 import statistics
 import subprocess
+import time
 import sys
 
 import numpy as np
@@ -279,6 +280,50 @@ def _screened_vs_plain(args, local_rank: int) -> dict:
         res["points"], res["dim"], res["eps"], res["steps"] = N, n, w.eps, args.sv_steps
         out[name] = res
         del tables
+    return out
+
+
+def _learned_vs_sampled(args, local_rank: int) -> dict:
+    """The 6-D workload's estimator comparison: the result-count model is
+    trained on the device on the exact per-cell counts of a join of the same
+    distribution at half size, then the full 5M-point join runs with the
+    sampled estimator and with the learned one (device-resident input, same
+    step counts); reported: each estimate, its error, its device time, the
+    join time, re-runs, and whether both joins gave the same lists."""
+    import torch
+
+    from gpu_self_join_b200 import JoinConfig, SelfJoin, synth
+
+    name = "c3_gmm6d"
+    w = synth.WORKLOADS[name]
+    cfg_s = JoinConfig(indexed_dims=w.k, reorder=w.reorder, shortcircuit=w.shortcircuit, ilp=w.ilp, stamp=w.stamp,
+                       query_reorder=w.query_reorder)
+    cfg_l = JoinConfig(indexed_dims=w.k, reorder=w.reorder, shortcircuit=w.shortcircuit, ilp=w.ilp, stamp=w.stamp,
+                       query_reorder=w.query_reorder, learned=True)
+    out = {"workload": name, "train_points": 2_500_000}
+    with SelfJoin(local_rank) as sj:
+        sj.run(torch.from_numpy(synth.generate(name, 2_500_000)).cuda(), w.eps, cfg_s)
+        t0 = time.perf_counter()
+        loss = sj.model_train(400)
+        out["train"] = {"steps": 400, "wall_ms": (time.perf_counter() - t0) * 1e3, "last_loss": loss}
+        x = torch.from_numpy(synth.generate(name)).cuda()
+        lists = {}
+        for arm, cfg in (("sampled", cfg_s), ("learned", cfg_l)):
+            sj.run(x, w.eps, cfg)  # warm-up
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            stats = [sj.run(x, w.eps, cfg) for _ in range(args.sv_steps)]
+            e1.record()
+            torch.cuda.synchronize()
+            s = stats[-1]
+            R = int(s["total_pairs"])
+            out[arm] = {"join_ms": e0.elapsed_time(e1) / args.sv_steps, "estimate": int(s["estimate"]),
+                        "estimate_error": (int(s["estimate"]) - R) / R, "estimate_dev_ms": s["dev_ms_estimate"],
+                        "reruns": int(s["reruns"]), "result_pairs": R}
+            lists[arm] = (sj.counts(), sj.table())
+    out["same_pairs"] = bool(np.array_equal(lists["sampled"][0], lists["learned"][0])
+                             and np.array_equal(lists["sampled"][1], lists["learned"][1]))
     return out
 
 
@@ -569,6 +614,10 @@ def _ours(args) -> None:
             line["screened_vs_plain"] = _screened_vs_plain(args, local_rank)
         except Exception as ex:  # reported, never required for the headline line
             line["screened_vs_plain"] = {"error": str(ex)}
+        try:
+            line["learned_vs_sampled"] = _learned_vs_sampled(args, local_rank)
+        except Exception as ex:  # reported, never fatal for the headline line
+            line["learned_vs_sampled"] = {"error": str(ex)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = _cpu_baseline(pts, w)
