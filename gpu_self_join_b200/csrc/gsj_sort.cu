@@ -7,7 +7,8 @@
 // points by cell with ties in ascending point id - the reference's per-cell
 // order (main.cu:741-763).
 //
-// Each 8-bit digit pass is a reduce-then-scan over tiles of kSortTile keys:
+// Each digit pass (8-bit digits, or 9-bit where that saves a pass) is a
+// reduce-then-scan over tiles of kSortTile keys:
 //   k_radix_hist     per-tile digit counts, written digit-major
 //   scan_u32_u32     exclusive scan of the counts: the global offset of each
 //                    (digit, tile) run
@@ -32,8 +33,8 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 8;                           // keys per thread
 constexpr int kSortTile = kSortThreads * kSortItems;    // keys per tile
 constexpr int kWarpKeys = kSortTile / kSortWarps;       // keys per warp (8 rounds of 32)
-constexpr int kBins = 256;
-static_assert(kSortThreads == kBins, "one thread per digit in the tile prefix");
+constexpr int kMaxBins = 512;  // digits of 8 or 9 bits
+static_assert(kMaxBins % kSortThreads == 0, "whole digits per thread in the tile prefix");
 
 __device__ __forceinline__ unsigned lanemask_lt_s() {
     unsigned m;
@@ -41,32 +42,34 @@ __device__ __forceinline__ unsigned lanemask_lt_s() {
     return m;
 }
 
-template <typename K>
+template <typename K, int BINS>
 __device__ __forceinline__ uint32_t digit_of(K key, int shift) {
-    return (uint32_t)(key >> shift) & (uint32_t)(kBins - 1);
+    return (uint32_t)(key >> shift) & (uint32_t)(BINS - 1);
 }
 
-template <typename K>
+template <typename K, int BINS>
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const K* __restrict__ keys, uint64_t n, int shift,
                                                              uint32_t* __restrict__ hist, uint32_t ntiles) {
-    __shared__ uint32_t h[kSortWarps][kBins];
-    for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&h[0][0])[i] = 0u;
+    __shared__ uint32_t h[kSortWarps][BINS];
+    for (int i = threadIdx.x; i < kSortWarps * BINS; i += kSortThreads) (&h[0][0])[i] = 0u;
     __syncthreads();
     const int warp = threadIdx.x >> 5;
     const uint64_t base = (uint64_t)blockIdx.x * kSortTile;
 #pragma unroll 4
     for (int i = 0; i < kSortItems; i++) {
         const uint64_t e = base + (uint64_t)i * kSortThreads + threadIdx.x;
-        if (e < n) atomicAdd(&h[warp][digit_of(keys[e], shift)], 1u);
+        if (e < n) atomicAdd(&h[warp][digit_of<K, BINS>(keys[e], shift)], 1u);
     }
     __syncthreads();
-    uint32_t s = 0;
+    for (int d = threadIdx.x; d < BINS; d += kSortThreads) {
+        uint32_t s = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; w++) s += h[w][threadIdx.x];
-    hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = s;
+        for (int w = 0; w < kSortWarps; w++) s += h[w][d];
+        hist[(uint64_t)d * ntiles + blockIdx.x] = s;
+    }
 }
 
-template <typename K, bool VALS>
+template <typename K, bool VALS, int BINS>
 __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const K* __restrict__ kin,
                                                                 const uint32_t* __restrict__ vin,
                                                                 K* __restrict__ kout, uint32_t* __restrict__ vout,
@@ -75,13 +78,14 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const K* __restr
     extern __shared__ __align__(16) unsigned char sort_smem[];
     K* skeys = reinterpret_cast<K*>(sort_smem);
     uint32_t* svals = reinterpret_cast<uint32_t*>(sort_smem + sizeof(K) * kSortTile);
-    __shared__ uint32_t wcnt[kSortWarps][kBins];  // per-warp digit counts, then their exclusive prefix
-    __shared__ uint32_t tile_off[kBins];           // exclusive prefix of the tile's digit counts
-    __shared__ uint32_t gbase[kBins];              // global offset of the digit's run minus tile_off
+    constexpr int DPT = BINS / kSortThreads;       // digits per thread in the tile prefix
+    __shared__ uint32_t wcnt[kSortWarps][BINS];    // per-warp digit counts, then their exclusive prefix
+    __shared__ uint32_t tile_off[BINS];            // exclusive prefix of the tile's digit counts
+    __shared__ uint32_t gbase[BINS];               // global offset of the digit's run minus tile_off
     __shared__ uint32_t wsum[kSortWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = lanemask_lt_s();
-    for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&wcnt[0][0])[i] = 0u;
+    for (int i = threadIdx.x; i < kSortWarps * BINS; i += kSortThreads) (&wcnt[0][0])[i] = 0u;
     __syncthreads();
 
     const uint64_t base = (uint64_t)blockIdx.x * kSortTile + (uint64_t)warp * kWarpKeys;
@@ -94,7 +98,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const K* __restr
         const bool valid = e < n;
         key[r] = valid ? kin[e] : K(0);
         if (VALS) val[r] = valid ? vin[e] : 0u;
-        const uint32_t d = valid ? digit_of(key[r], shift) : (uint32_t)kBins;
+        const uint32_t d = valid ? digit_of<K, BINS>(key[r], shift) : (uint32_t)BINS;
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         const int leader = __ffs(peers) - 1;
         uint32_t c = 0;
@@ -107,15 +111,23 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const K* __restr
         __syncwarp();
     }
     __syncthreads();
-    // per digit (one thread each): prefix over the warps, then over the digits
+    // per digit (DPT consecutive digits a thread): prefix over the warps, then
+    // over the digits
     {
-        const int d = threadIdx.x;
+        const int d0 = threadIdx.x * DPT;
+        uint32_t pd[DPT];
         uint32_t p = 0;
 #pragma unroll
-        for (int w = 0; w < kSortWarps; w++) {
-            const uint32_t t = wcnt[w][d];
-            wcnt[w][d] = p;
-            p += t;
+        for (int dd = 0; dd < DPT; dd++) {
+            uint32_t q = 0;
+#pragma unroll
+            for (int w = 0; w < kSortWarps; w++) {
+                const uint32_t t = wcnt[w][d0 + dd];
+                wcnt[w][d0 + dd] = q;
+                q += t;
+            }
+            pd[dd] = q;
+            p += q;
         }
         uint32_t x = p;
 #pragma unroll
@@ -129,15 +141,20 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const K* __restr
 #pragma unroll
         for (int w = 0; w < kSortWarps; w++)
             if (w < warp) before += wsum[w];
-        const uint32_t ex = before + x - p;
-        tile_off[d] = ex;
-        gbase[d] = offs[(uint64_t)d * ntiles + blockIdx.x] - ex;  // modulo 2^32, re-added below
+        uint32_t ex = before + x - p;
+#pragma unroll
+        for (int dd = 0; dd < DPT; dd++) {
+            const int d = d0 + dd;
+            tile_off[d] = ex;
+            gbase[d] = offs[(uint64_t)d * ntiles + blockIdx.x] - ex;  // modulo 2^32, re-added below
+            ex += pd[dd];
+        }
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; r++) {
         const uint32_t d = rank[r] >> 16;
-        if (d < (uint32_t)kBins) {
+        if (d < (uint32_t)BINS) {
             const uint32_t idx = tile_off[d] + wcnt[warp][d] + (rank[r] & 0xffffu);
             skeys[idx] = key[r];
             if (VALS) svals[idx] = val[r];
@@ -148,7 +165,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const K* __restr
     const uint32_t cnt = (uint32_t)((n - tbase) < (uint64_t)kSortTile ? (n - tbase) : (uint64_t)kSortTile);
     for (uint32_t i = threadIdx.x; i < cnt; i += kSortThreads) {
         const K kk = skeys[i];
-        const uint32_t g = gbase[digit_of(kk, shift)] + i;
+        const uint32_t g = gbase[digit_of<K, BINS>(kk, shift)] + i;
         kout[g] = kk;
         if (VALS) vout[g] = svals[i];
     }
@@ -180,9 +197,9 @@ inline uint64_t tiles_of(uint64_t n) { return (n + kSortTile - 1) / kSortTile; }
 
 size_t radix_sort_temp_bytes(uint64_t n) {
     const uint64_t nt = tiles_of(n);
-    const size_t hist = (size_t)kBins * nt * sizeof(uint32_t);
+    const size_t hist = (size_t)kMaxBins * nt * sizeof(uint32_t);
     const size_t hist_al = (2 * hist + sizeof(uint32_t) + 255) / 256 * 256;
-    return hist_al + scan_u32_u64_temp_bytes((uint64_t)kBins * nt) + 256;
+    return hist_al + scan_u32_u64_temp_bytes((uint64_t)kMaxBins * nt) + 256;
 }
 
 template <typename K>
@@ -192,28 +209,44 @@ cudaError_t radix_sort(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt,
     if (n <= 1 || begin_bit >= end_bit) return cudaSuccess;
     if (n >= (1ull << 32)) return cudaErrorInvalidValue;
     const uint64_t nt = tiles_of(n);
-    const size_t hist_bytes = (size_t)kBins * nt * sizeof(uint32_t);
+    const size_t hist_bytes = (size_t)kMaxBins * nt * sizeof(uint32_t);
     uint32_t* hist = static_cast<uint32_t*>(temp);
     uint32_t* offs = reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(temp) + hist_bytes);
     void* stemp = static_cast<unsigned char*>(temp) + (2 * hist_bytes + sizeof(uint32_t) + 255) / 256 * 256;
     const size_t smem = sizeof(K) * kSortTile + (vals ? sizeof(uint32_t) * kSortTile : 0);
-    auto kv = k_radix_scatter<K, true>;
-    auto kk = k_radix_scatter<K, false>;
-    cudaError_t e = cudaFuncSetAttribute(vals ? (const void*)kv : (const void*)kk,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    cudaError_t e;
+    for (const void* f : {(const void*)k_radix_scatter<K, true, 256>, (const void*)k_radix_scatter<K, false, 256>,
+                          (const void*)k_radix_scatter<K, true, 512>, (const void*)k_radix_scatter<K, false, 512>}) {
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    // digits of 8 bits, or of 9 where that saves a pass (25 key bits: 9 + 8 + 8)
+    const int B = end_bit - begin_bit;
+    const int p8 = (B + 7) / 8, p9 = (B + 8) / 9;
+    const int passes = p9 < p8 ? p9 : p8;
+    const int nine = p9 < p8 ? B - 8 * passes : 0;  // passes with 9-bit digits
     K *ki = keys, *ko = keys_alt;
     uint32_t *vi = vals, *vo = vals_alt;
     bool alt = false;
-    for (int shift = begin_bit; shift < end_bit; shift += 8) {
-        k_radix_hist<K><<<(unsigned)nt, kSortThreads, 0, st>>>(ki, n, shift, hist, (uint32_t)nt);
-        e = scan_u32_u32(hist, offs, (uint64_t)kBins * nt, stemp, st);
+    int shift = begin_bit;
+    for (int pass = 0; pass < passes; pass++) {
+        const bool wide = pass < nine;
+        const uint32_t bins = wide ? 512u : 256u;
+        if (wide) k_radix_hist<K, 512><<<(unsigned)nt, kSortThreads, 0, st>>>(ki, n, shift, hist, (uint32_t)nt);
+        else k_radix_hist<K, 256><<<(unsigned)nt, kSortThreads, 0, st>>>(ki, n, shift, hist, (uint32_t)nt);
+        e = scan_u32_u32(hist, offs, (uint64_t)bins * nt, stemp, st);
         if (e != cudaSuccess) return e;
-        if (vals) kv<<<(unsigned)nt, kSortThreads, smem, st>>>(ki, vi, ko, vo, n, shift, offs, (uint32_t)nt);
-        else kk<<<(unsigned)nt, kSortThreads, smem, st>>>(ki, nullptr, ko, nullptr, n, shift, offs, (uint32_t)nt);
+        if (wide) {
+            if (vals) k_radix_scatter<K, true, 512><<<(unsigned)nt, kSortThreads, smem, st>>>(ki, vi, ko, vo, n, shift, offs, (uint32_t)nt);
+            else k_radix_scatter<K, false, 512><<<(unsigned)nt, kSortThreads, smem, st>>>(ki, nullptr, ko, nullptr, n, shift, offs, (uint32_t)nt);
+        } else {
+            if (vals) k_radix_scatter<K, true, 256><<<(unsigned)nt, kSortThreads, smem, st>>>(ki, vi, ko, vo, n, shift, offs, (uint32_t)nt);
+            else k_radix_scatter<K, false, 256><<<(unsigned)nt, kSortThreads, smem, st>>>(ki, nullptr, ko, nullptr, n, shift, offs, (uint32_t)nt);
+        }
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (launches) *launches += 5;
+        shift += wide ? 9 : 8;
         K* tk = ki;
         ki = ko;
         ko = tk;
