@@ -33,12 +33,14 @@
 // only make the test inconclusive, which sends the pair to the exact check.
 //
 // Synchronisation: warps 8-11 produce candidate tiles (slot search, cp.async of
-// the rows) and issue the MMA, warps 0-7 consume; candidate tiles rotate
-// through kStages buffers and two accumulators alternate, handed over by
-// mbarriers (full: MMA commit + the issuer's release; empty: the consumer
-// arrivals).  Every wait is a bounded poll by one thread whose verdict is
-// shared before any barrier or warp-collective; on time-out the error flag is
-// raised and the CTA stops.  Tensor memory (2 x 128 columns) is allocated once
+// the rows) and one of their threads issues the MMA, warps 0-7 consume;
+// candidate tiles rotate through kStages buffers and two accumulators
+// alternate, handed over by mbarriers only (staged: every producer thread's
+// slots and landed rows of a buffer; full: MMA commit + the issuer's release;
+// empty and free: the consumer arrivals), so the producer warps never wait for
+// one another.  Every wait is a bounded poll by one thread whose verdict is
+// shared before any warp-collective; on time-out the error flag is raised and
+// the CTA stops.  Tensor memory (2 x 128 columns) is allocated once
 // per CTA; the shared-memory request keeps at most 2 CTAs (512 columns) on an
 // SM; it is released before exit.
 #include <algorithm>
@@ -255,30 +257,12 @@ __device__ __forceinline__ void bar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ void named_sync(uint32_t id, uint32_t count) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
-}
-
-// Barrier among `count` threads that also returns the OR of their flags, so a
-// decision taken after it is the same in every participating thread.
-__device__ __forceinline__ bool named_sync_or(uint32_t id, uint32_t count, bool flag) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, %3, p;\n\t"
-        "selp.u32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(r)
-        : "r"((uint32_t)flag), "r"(id), "r"(count)
-        : "memory");
-    return r != 0u;
-}
-
 // The CTA is warp-specialised: warps 8-11 produce (candidate slots, centred
 // BF16 candidate rows with the norm folded in, the MMA), warps 0-7 consume
 // (tensor-memory rows, the screen, the undecided-pair appends).  Candidate
 // tiles rotate through kStages buffers and two accumulators alternate;
-// mbarriers full[s] (MMA done) and empty[s] (accumulator read) hand them over.
+// mbarriers staged[b] (rows in place), full[s] (MMA done), empty[s]
+// (accumulator read) and free[b] (buffer read) hand them over.
 //
 // With the norm folded into the product (A row, the query = [-2 q^, 1, 1];
 // B row, the candidate = [c^, |c^|^2_hi, |c^|^2_lo]), the accumulator holds
@@ -305,6 +289,7 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
     const uint32_t full0 = smem_u32(misc + 24), full1 = smem_u32(misc + 26);
     const uint32_t empty0 = smem_u32(misc + 28), empty1 = smem_u32(misc + 30);
     const uint32_t free0 = smem_u32(misc + 32);  // free_b = free0 + 8 b
+    const uint32_t staged0 = smem_u32(misc + 38);  // staged_b = staged0 + 8 b
 
     // ---- set-up: mbarriers, tensor memory (two accumulators)
     if (tid == 0) {
@@ -317,6 +302,9 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
         // free[b]: the consumers are done with stage b (candidate tile, slots, norm bound)
         for (uint32_t b = 0; b < kStages; b++)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 256;" ::"r"(free0 + 8u * b) : "memory");
+        // staged[b]: the 128 producer threads' slots and rows of stage b are in place
+        for (uint32_t b = 0; b < kStages; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(staged0 + 8u * b) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -435,17 +423,21 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
 
         if (tid >= kProd0) {
             // ================= producer warps: stage tile t + 1 (slots, cp.async of
-            // the rows) before completing tile t (copies landed, MMA issued)
+            // the rows) before publishing tile t (copies landed); one thread then
+            // issues tile t's MMA
             const uint32_t pt = (uint32_t)tid - (uint32_t)kProd0;  // candidate row of the tile
-            // the copy walks (row, chunk) pairs in row-major order, 128 apart
-            const uint32_t step_r = (uint32_t)kSC / kch, step_c = (uint32_t)kSC % kch;
             uint32_t e = 0;  // neighbour range of this thread's current candidate (f grows by kSC per tile)
             float wm_cur = 0.f, wm_next = 0.f;  // candidate norms of the last two prepared tiles
+            const uint32_t wbase = (uint32_t)(warp - 8) * 32u;  // this warp's first row of the tile
+            // stage tile t: this warp's 32 slots and rows (no barrier with the other
+            // producer warps: the stage is free once its consumers released it)
             auto prepare = [&](uint32_t t) -> bool {
                 const uint32_t g = tiles_done + t, b = g % kStages;
-                bool bad = false;
-                if (g >= kStages && pt == 0) bad = !bar_wait_bounded(free0 + 8u * b, ((g / kStages) - 1u) & 1u);
-                if (named_sync_or(1, 128, bad)) return false;
+                if (g >= kStages) {
+                    bool ok = true;
+                    if (lane == 0) ok = bar_wait_bounded(free0 + 8u * b, ((g / kStages) - 1u) & 1u);
+                    if (!__shfl_sync(FULL, ok ? 1u : 0u, 0)) return false;
+                }
                 const uint32_t f = t * kSC + pt;
                 uint32_t slot = kNone;
                 wm_cur = wm_next;
@@ -454,41 +446,35 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                     while (nb_pref[e + 1] <= f) e++;
                     slot = nb_start[e] + (f - nb_pref[e]);
                     // |c^|^2 in FP32 bounds the folded hi + lo terms (reduced when the
-                    // tile is completed, so that the load's latency is not waited for here)
+                    // tile is published, so that the load's latency is not waited for here)
                     wm_next = sc.norms[slot];
                 }
                 c_slot[b * kSC + pt] = slot;
                 const uint32_t dst = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
                 if (kch <= 4u) {
-                    // short rows (up to 32 values): each thread copies its own row, no barrier
+                    // short rows (up to 32 values): each thread copies its own row
                     const bool valid = slot != kNone;
                     const uint4* src = sc.rows + (size_t)(valid ? slot : 0u) * kch;
                     for (uint32_t kc = 0; kc < kch; kc++)
                         cp_async16(dst + core_off(pt, kc, kpad), src + kc, valid ? 16u : 0u);
-                    asm volatile("cp.async.commit_group;" ::: "memory");
                 } else {
-                    // longer rows: consecutive threads copy consecutive chunks of a row
-                    named_sync(1, 128);
-                    uint32_t r = pt / kch, kc = pt % kch;
+                    // longer rows: the warp's 32 rows, consecutive lanes on consecutive
+                    // chunks of a row
                     for (uint32_t j = 0; j < kch; j++) {
-                        const uint32_t sl = c_slot[b * kSC + r];
+                        const uint32_t idx = j * 32u + (uint32_t)lane;
+                        const uint32_t r = idx / kch, kc = idx - r * kch;
+                        const uint32_t sl = __shfl_sync(FULL, slot, (int)r);
                         const bool valid = sl != kNone;
-                        cp_async16(dst + core_off(r, kc, kpad), sc.rows + (size_t)(valid ? sl : 0u) * kch + kc,
-                                   valid ? 16u : 0u);
-                        r += step_r;
-                        kc += step_c;
-                        if (kc >= kch) {
-                            kc -= kch;
-                            r++;
-                        }
+                        cp_async16(dst + core_off(wbase + r, kc, kpad),
+                                   sc.rows + (size_t)(valid ? sl : 0u) * kch + kc, valid ? 16u : 0u);
                     }
-                    asm volatile("cp.async.commit_group;" ::: "memory");
                 }
+                asm volatile("cp.async.commit_group;" ::: "memory");
                 return true;
             };
-            auto complete = [&](uint32_t t, bool next_pending) -> bool {
-                const uint32_t g = tiles_done + t, b = g % kStages, s = g & 1u;
-                // tile t's norms: loaded by prepare(t), i.e. wm_cur once prepare(t + 1) ran
+            // tile t's rows landed (this thread's copies): publish slots, norm bound and rows
+            auto publish = [&](uint32_t t, bool next_pending) {
+                const uint32_t g = tiles_done + t, b = g % kStages;
                 float wm = next_pending ? wm_cur : wm_next;
 #pragma unroll
                 for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
@@ -496,32 +482,40 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 if (next_pending) asm volatile("cp.async.wait_group 1;" ::: "memory");
                 else asm volatile("cp.async.wait_group 0;" ::: "memory");
                 fence_async_smem();
-                bool bad = false;
-                if (g >= 2 && pt == 0) bad = !bar_wait_bounded((s ? empty1 : empty0), ((g >> 1) - 1u) & 1u);
-                if (named_sync_or(1, 128, bad)) return false;
-                if (pt == 0) {
-                    // the tile's largest candidate norm and its square root (rounded up), for all consumers
-                    const float cmax = fmaxf(fmaxf(cwmax[b * 4u], cwmax[b * 4u + 1u]),
-                                             fmaxf(cwmax[b * 4u + 2u], cwmax[b * 4u + 3u]));
-                    cwmax[b * 4u] = cmax;
-                    cwmax[b * 4u + 1u] = __fsqrt_ru(cmax);
-                    fence_after();
-                    const uint32_t b_addr = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
-                    for (uint32_t ks = 0; ks < (kpad >> 4); ks++)
-                        mma_bf16(tmem + s * kTmemCols, smem_desc(a_addr + ks * 256u, 128u, sbo),
-                                 smem_desc(b_addr + ks * 256u, 128u, sbo), ks > 0 ? 1u : 0u);
-                    mma_commit((s ? full1 : full0));
-                    bar_arrive((s ? full1 : full0));
-                }
+                bar_arrive(staged0 + 8u * b);
+            };
+            // one thread: tile t staged by all producers and its accumulator free -> MMA
+            auto issue = [&](uint32_t t) -> bool {
+                const uint32_t g = tiles_done + t, b = g % kStages, s = g & 1u;
+                if (!bar_wait_bounded(staged0 + 8u * b, (g / kStages) & 1u)) return false;
+                if (g >= 2 && !bar_wait_bounded((s ? empty1 : empty0), ((g >> 1) - 1u) & 1u)) return false;
+                // the tile's largest candidate norm and its square root (rounded up), for all consumers
+                const float cmax = fmaxf(fmaxf(cwmax[b * 4u], cwmax[b * 4u + 1u]),
+                                         fmaxf(cwmax[b * 4u + 2u], cwmax[b * 4u + 3u]));
+                cwmax[b * 4u] = cmax;
+                cwmax[b * 4u + 1u] = __fsqrt_ru(cmax);
+                fence_after();
+                const uint32_t b_addr = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
+                for (uint32_t ks = 0; ks < (kpad >> 4); ks++)
+                    mma_bf16(tmem + s * kTmemCols, smem_desc(a_addr + ks * 256u, 128u, sbo),
+                             smem_desc(b_addr + ks * 256u, 128u, sbo), ks > 0 ? 1u : 0u);
+                mma_commit((s ? full1 : full0));
+                bar_arrive((s ? full1 : full0));
                 return true;
             };
             bool ok = T == 0 || prepare(0);
             for (uint32_t t = 0; ok && t < T; t++) {
                 if (t + 1 < T) ok = prepare(t + 1);
-                if (ok) ok = complete(t, t + 1 < T);
+                if (!ok) break;
+                publish(t, t + 1 < T);
+                if (warp == 8) {
+                    bool r = true;
+                    if (lane == 0) r = issue(t);
+                    ok = __shfl_sync(FULL, r ? 1u : 0u, 0) != 0u;
+                }
             }
             asm volatile("cp.async.wait_all;" ::: "memory");
-            if (!ok && pt == 0) misc[1] = 1u;
+            if (!ok) misc[1] = 1u;
         } else {
             // ================= consumer warps: query row i = TMEM lane i; warps w and
             // w + 4 share lane quarter w % 4 and split the columns
