@@ -18,7 +18,8 @@
 //      BF16 products; -2 q^ is exact in BF16).
 //   3. Every consumer thread reads its query's row (tcgen05.ld 32x32b) and
 //      rejects candidate j when that value exceeds
-//      G_i = (R0 + kE (|q^_i| + max_j |c^_j|))^2 + c1 (|q^_i|^2 + 2 max_j |c^_j|^2) - |q^_i|^2.
+//      G_i = (R0 + kE (|q^_i| + max_j |c^_j|))^2 + c1 (|q^_i|^2 + 2 max_j |c^_j|^2) - |q^_i|^2,
+//      the maximum over the 32 candidates of j's column group.
 //      The bound is proven, not tuned: R0^2 covers the rounding of the
 //      reference's own FP32 sum (at most 2n+8 roundings of non-negative
 //      terms), kE the BF16 rounding of both centred points and of the centring
@@ -235,8 +236,8 @@ __host__ __device__ inline ScreenSmem screen_smem(uint32_t kpad, uint32_t noff) 
     o = (o + 15u) & ~15u;
     t.cslot = o;  // [kStages][kSC]
     o += kStages * kSC * 4u;
-    t.cwmax = o;  // [kStages][4] largest candidate norm per producer warp
-    o += kStages * 4u * 4u;
+    t.cwmax = o;  // [kStages][8] per 32-candidate group: largest norm [0..3], its square root [4..7]
+    o += kStages * 8u * 4u;
     t.qid = o;
     o += kSQ * 4u;
     o = (o + 15u) & ~15u;
@@ -478,7 +479,10 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 float wm = next_pending ? wm_cur : wm_next;
 #pragma unroll
                 for (int sh = 16; sh > 0; sh >>= 1) wm = fmaxf(wm, __shfl_xor_sync(FULL, wm, sh));
-                if (lane == 0) cwmax[b * 4u + (uint32_t)(warp - 8)] = wm;
+                if (lane == 0) {
+                    cwmax[b * 8u + (uint32_t)(warp - 8)] = wm;
+                    cwmax[b * 8u + 4u + (uint32_t)(warp - 8)] = __fsqrt_ru(wm);
+                }
                 if (next_pending) asm volatile("cp.async.wait_group 1;" ::: "memory");
                 else asm volatile("cp.async.wait_group 0;" ::: "memory");
                 fence_async_smem();
@@ -489,11 +493,6 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 const uint32_t g = tiles_done + t, b = g % kStages, s = g & 1u;
                 if (!bar_wait_bounded(staged0 + 8u * b, (g / kStages) & 1u)) return false;
                 if (g >= 2 && !bar_wait_bounded((s ? empty1 : empty0), ((g >> 1) - 1u) & 1u)) return false;
-                // the tile's largest candidate norm and its square root (rounded up), for all consumers
-                const float cmax = fmaxf(fmaxf(cwmax[b * 4u], cwmax[b * 4u + 1u]),
-                                         fmaxf(cwmax[b * 4u + 2u], cwmax[b * 4u + 3u]));
-                cwmax[b * 4u] = cmax;
-                cwmax[b * 4u + 1u] = __fsqrt_ru(cmax);
                 fence_after();
                 const uint32_t b_addr = smem_u32(ssm + L.b) + b * ((uint32_t)kSC * kpad * 2u);
                 for (uint32_t ks = 0; ks < (kpad >> 4); ks++)
@@ -534,16 +533,17 @@ __global__ void __launch_bounds__(kSThreads, 2) k_tile_screen(const JoinArgs<flo
                 }
                 fence_after();
                 const uint32_t b = g % kStages;
-                const float cmax = cwmax[b * 4u], rcmax = cwmax[b * 4u + 1u];
-                // G_i from the tile's largest candidate norm (an upper bound of every column's bound)
-                const float tt = __fmaf_ru(sc.ke, rcmax, qi.y);
-                const float G =
-                    __fsub_ru(__fmaf_ru(tt, tt, __fadd_ru(qi.z, __fmul_ru(sc.c1, __fmul_ru(2.f, cmax)))), qi.x);
                 const uint32_t nvalid = min((uint32_t)kSC, total - t * kSC);
                 // a warp whose 32 query rows are all empty still waits for every tile
                 // (its arrivals keep the phases of empty[] in order) but skips the work
                 const uint32_t col_end = (quarter * 32u < qn) ? colbase + (uint32_t)kSC / 2u : colbase;
                 for (uint32_t c32 = colbase; c32 < col_end; c32 += 32u) {
+                  // G_i from the group's largest candidate norm (an upper bound of each of
+                  // its 32 columns' bounds; the group's candidates are one producer warp's)
+                  const float cmax = cwmax[b * 8u + (c32 >> 5)], rcmax = cwmax[b * 8u + 4u + (c32 >> 5)];
+                  const float tt = __fmaf_ru(sc.ke, rcmax, qi.y);
+                  const float G =
+                      __fsub_ru(__fmaf_ru(tt, tt, __fadd_ru(qi.z, __fmul_ru(sc.c1, __fmul_ru(2.f, cmax)))), qi.x);
                   float d32[32];
                   tmem_ld32(tmem + s * kTmemCols + ((quarter * 32u) << 16) + c32, d32);
                   // common case: every value of the 32 columns above G (NaN counts as undecided)
