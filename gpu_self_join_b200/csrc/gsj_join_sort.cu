@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(128) k_sort_join(const JoinArgs<T> a, const ui
             cand++;
             const T d2 = sqdist_lane<T, MODEL, POL>(p, a.pts + (size_t)slot * npad, n, a.ilp);
             if (d2 <= thr) {
-                if (FILL) {
+                if constexpr (FILL) {
                     if (cnt < len_cap) list[cnt] = a.ids[slot];
                     else *a.err_flag = 1u;
                 }
