@@ -13,13 +13,13 @@
 //                 reference's arithmetic and records the decisions as a bit
 //                 mask (bit f of the query's words), the list length by slot and
 //                 by point id.
-//   k_rows_fill   a warp per 32 consecutive query slots, the queries taken one
-//                 after another.  The warp replays the query's bit mask - no
-//                 second distance pass - 32 candidates per mask word: lane j
-//                 takes bit j, loads the id of its candidate when the bit is set,
-//                 and stores it at the query's next free list position, so each
-//                 word's hits are written by consecutive lanes to consecutive
-//                 places of the point-id-ordered table.
+//   k_rows_fill   a warp per 32 consecutive query slots, two queries at a time
+//                 (one per half-warp).  A half-warp replays its query's bit mask
+//                 - no second distance pass - one mask word per step: lane l
+//                 takes bits 2l and 2l + 1, loads the ids of those candidates
+//                 whose bit is set, and stores them at the query's next free list
+//                 positions, so each word's hits are written by the half's lanes
+//                 to consecutive places of the point-id-ordered table.
 // Both kernels claim their 32-slot chunks dynamically (one atomic per warp,
 // the next claim issued before the current chunk is processed), since chunk
 // costs vary with the local density by orders of magnitude.
@@ -135,12 +135,6 @@ __global__ void __launch_bounds__(256) k_rows_count(const JoinArgs<T> a, const u
     if (lane == 0 && cand) atomicAdd(a.cand_cnt, cand);
 }
 
-__device__ __forceinline__ unsigned lanemask_lt_q() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
 // Queries: the slots qslots[0 .. nq) (all slots 0 .. nq-1 when qslots is
 // null); the list of point id i goes to a.table[offsets[i] - base].
 // Per-query parameters of the fill, staged in shared memory by the lane that
@@ -163,7 +157,6 @@ __global__ void __launch_bounds__(256) k_rows_fill(const JoinArgs<float> a, cons
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     FillQuery<NR>* wq = qp[threadIdx.x >> 5];
-    const unsigned lt = lanemask_lt_q();
     uint32_t cur = __shfl_sync(FULL, claim32(a.work_counter, lane), 0);
     while (cur < nq) {
         const uint32_t nxt = claim32(a.work_counter, lane);
@@ -194,39 +187,35 @@ __global__ void __launch_bounds__(256) k_rows_fill(const JoinArgs<float> a, cons
         __syncwarp();  // the previous chunk's reads of wq are done
         wq[lane] = f;
         __syncwarp();
-        for (uint32_t qi = 0; qi < nv; qi++) {
-            const FillQuery<NR> q = wq[qi];
-            if (q.cnt == 0u) continue;
+        // two queries at a time, one per half-warp: lane l of a half takes bits
+        // 2l and 2l + 1 of each of its query's mask words
+        const uint32_t h = (uint32_t)lane >> 4, hl = (uint32_t)lane & 15u;
+        for (uint32_t qi = 0; qi < nv; qi += 2u) {
+            const FillQuery<NR> q = wq[qi + h];  // entries past nv are zero (no words)
+            const uint32_t qnw = q.cnt ? q.nw : 0u;
             uint32_t* list = a.table + q.dst;
             const uint32_t* qb = bits + q.bo;
-            uint32_t run = 0;  // entries of the list written so far
-            for (uint32_t t0 = 0; t0 < q.nw && run < q.cnt; t0 += 32u) {
-                const uint32_t myw = (t0 + (uint32_t)lane < q.nw) ? qb[t0 + lane] : 0u;
-                const uint32_t tn = min(32u, q.nw - t0);
-                // two mask words (64 candidates) per step
-                for (uint32_t tt = 0; tt < tn; tt += 2u) {
-                    const uint32_t w0 = __shfl_sync(FULL, myw, tt);
-                    uint32_t w1 = __shfl_sync(FULL, myw, (tt + 1u) & 31u);
-                    if (tt + 1u >= tn) w1 = 0u;
-                    if ((w0 | w1) == 0u) continue;
-                    const uint32_t p0 = (uint32_t)__popc(w0);
-                    const uint32_t f0 = (t0 + tt) * 32u + (uint32_t)lane;
-                    if ((w0 >> lane) & 1u) {
-                        uint32_t st = q.lo[0] + f0;
+            const uint32_t nwmax = max(__shfl_sync(FULL, qnw, 0), __shfl_sync(FULL, qnw, 16));
+            uint32_t run = 0;  // entries of this half's list written so far
+            for (uint32_t t0 = 0; t0 < nwmax; t0 += 16u) {
+                const uint32_t myw = (t0 + hl < qnw) ? qb[t0 + hl] : 0u;
+                const uint32_t tn = min(16u, nwmax - t0);
+                for (uint32_t tt = 0; tt < tn; tt++) {
+                    const uint32_t w = __shfl_sync(FULL, myw, (int)(h * 16u + tt));
+                    if (__ballot_sync(FULL, w != 0u) == 0u) continue;
 #pragma unroll
-                        for (int r = 1; r < NR; r++)
-                            if (f0 >= q.pre[r]) st = q.lo[r] + (f0 - q.pre[r]);
-                        list[run + (uint32_t)__popc(w0 & lt)] = a.ids[st];
-                    }
-                    if ((w1 >> lane) & 1u) {
-                        const uint32_t f1 = f0 + 32u;
-                        uint32_t st = q.lo[0] + f1;
+                    for (uint32_t bs = 0; bs < 2u; bs++) {
+                        const uint32_t bit = 2u * hl + bs;
+                        if ((w >> bit) & 1u) {
+                            const uint32_t f = (t0 + tt) * 32u + bit;
+                            uint32_t st = q.lo[0] + f;
 #pragma unroll
-                        for (int r = 1; r < NR; r++)
-                            if (f1 >= q.pre[r]) st = q.lo[r] + (f1 - q.pre[r]);
-                        list[run + p0 + (uint32_t)__popc(w1 & lt)] = a.ids[st];
+                            for (int r = 1; r < NR; r++)
+                                if (f >= q.pre[r]) st = q.lo[r] + (f - q.pre[r]);
+                            list[run + (uint32_t)__popc(w & ((1u << bit) - 1u))] = a.ids[st];
+                        }
                     }
-                    run += p0 + (uint32_t)__popc(w1);
+                    run += (uint32_t)__popc(w);
                 }
             }
         }
