@@ -55,9 +55,14 @@ def test_learned_estimate_gain_6d():
         sj.run(synth.generate("c3_gmm6d", 2_500_000), w.eps, cfg)
         sj.model_train(400)
         full = synth.generate("c3_gmm6d")
+        # each estimator's second full-size join is compared (the first one
+        # allocates the buffers it needs)
+        sj.run(full, w.eps, cfg)
         s_samp = sj.run(full, w.eps, cfg)
         c0, t0 = sj.counts(), sj.table()
-        s_learn = sj.run(full, w.eps, JoinConfig(indexed_dims=6, stamp=True, learned=True))
+        lcfg = JoinConfig(indexed_dims=6, stamp=True, learned=True)
+        sj.run(full, w.eps, lcfg)
+        s_learn = sj.run(full, w.eps, lcfg)
         c1, t1 = sj.counts(), sj.table()
     assert np.array_equal(c0, c1) and np.array_equal(t0, t1)
     R = s_learn["total_pairs"]
