@@ -60,20 +60,37 @@ class ClockSampler:
         self.lines: list[str] = []
         self.path = None
 
+    def _lines(self) -> int:
+        try:
+            with open(self.path) as f:
+                return sum(1 for ln in f if ln.strip())
+        except OSError:
+            return 0
+
     def start(self):
+        """Starts sampling every 50 ms and returns once the first sample is
+        written, so that a short timed region is still covered."""
         import tempfile
 
         self.path = tempfile.mktemp(suffix=".csv")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100", "-f", self.path],
+                                          "--format=csv,noheader,nounits", "-lms", "50", "-f", self.path],
                                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t_end = time.time() + 3.0
+        while time.time() < t_end and self.proc.poll() is None and self._lines() == 0:
+            time.sleep(0.01)
 
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        # one more sample taken at or after the end of the timed region
+        n0, t_end = self._lines(), time.time() + 0.5
+        while time.time() < t_end and self.proc.poll() is None and self._lines() <= n0:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
