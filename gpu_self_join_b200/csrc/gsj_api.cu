@@ -1204,46 +1204,52 @@ int run_join(gsj_context* c, const void* data, uint64_t N, double eps_d, const g
         }
     }
 
-    // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525)
-    uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
-    GSJ_TRY(dev_get(c, c->nchunks, M + 1, &nchunks));
-    GSJ_TRY(dev_get(c, c->item_off, M + 1, &item_off));
-    if (cfg.query_reorder) {
-        uint32_t *sizes = nullptr, *sizes2 = nullptr, *iota = nullptr;
-        GSJ_TRY(dev_get(c, c->sizes, 2 * (size_t)M, &sizes));
-        sizes2 = sizes + M;
-        GSJ_TRY(dev_get(c, c->order, 2 * (size_t)M, &order));
-        iota = order + M;
-        // stable descending sort by cell size (ties keep ascending cell order):
-        // an ascending sort of the complemented sizes
-        S.kernel_launches += 2;
-        GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, sizes, st));
-        GSJ_CUDA(c, launch_iota(iota, M, st));
-        GSJ_TRY(dev_get(c, c->temp, radix_sort_temp_bytes(M), (unsigned char**)&temp));
-        bool alt = false;
-        int nl2 = 0;
-        GSJ_CUDA(c, radix_sort<uint32_t>(sizes, sizes2, iota, order, M, 0, 32, temp, &alt, &nl2, st));
-        S.kernel_launches += (uint64_t)nl2;
-        if (!alt) {
-            // the sorted cell indices are in iota (order + M): move them to order[0, M)
-            GSJ_CUDA(c, cudaMemcpyAsync(order, iota, (size_t)M * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-        }
-        S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_item_counts(cell_start, order, M, qchunk, nchunks, nullptr, st));
-    } else {
-        S.kernel_launches += 1;
-        GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, nullptr, st));
-    }
-    GSJ_TRY(dev_get(c, c->temp, scan_u32_u64_temp_bytes(M), (unsigned char**)&temp));
-    S.kernel_launches += 3;
-    GSJ_CUDA(c, scan_u32_u32(nchunks, item_off, M, temp, st));
+    // ---- work items (QUERYREORDER: heaviest cells first, GPU.cu:1491-1525).
+    // The ROWS path has none: its passes claim 32 consecutive query slots at a
+    // time, and the order in which queries run changes no result.
     uint32_t num_items = 0;
-    GSJ_TRY(d2h_small(c, &num_items, item_off + M, 1));
-    S.work_items = num_items;
     uint2* items = nullptr;
-    GSJ_TRY(dev_get(c, c->items, num_items, &items));
-    S.kernel_launches += 1;
-    GSJ_CUDA(c, launch_make_items(order, nchunks, item_off, M, items, st));
+    if (tpq) {
+        S.work_items = ((uint64_t)N + 31u) / 32u;
+    } else {
+        uint32_t *order = nullptr, *nchunks = nullptr, *item_off = nullptr;
+        GSJ_TRY(dev_get(c, c->nchunks, M + 1, &nchunks));
+        GSJ_TRY(dev_get(c, c->item_off, M + 1, &item_off));
+        if (cfg.query_reorder) {
+            uint32_t *sizes = nullptr, *sizes2 = nullptr, *iota = nullptr;
+            GSJ_TRY(dev_get(c, c->sizes, 2 * (size_t)M, &sizes));
+            sizes2 = sizes + M;
+            GSJ_TRY(dev_get(c, c->order, 2 * (size_t)M, &order));
+            iota = order + M;
+            // stable descending sort by cell size (ties keep ascending cell order):
+            // an ascending sort of the complemented sizes
+            S.kernel_launches += 2;
+            GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, sizes, st));
+            GSJ_CUDA(c, launch_iota(iota, M, st));
+            GSJ_TRY(dev_get(c, c->temp, radix_sort_temp_bytes(M), (unsigned char**)&temp));
+            bool alt = false;
+            int nl2 = 0;
+            GSJ_CUDA(c, radix_sort<uint32_t>(sizes, sizes2, iota, order, M, 0, 32, temp, &alt, &nl2, st));
+            S.kernel_launches += (uint64_t)nl2;
+            if (!alt) {
+                // the sorted cell indices are in iota (order + M): move them to order[0, M)
+                GSJ_CUDA(c, cudaMemcpyAsync(order, iota, (size_t)M * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+            }
+            S.kernel_launches += 1;
+            GSJ_CUDA(c, launch_item_counts(cell_start, order, M, qchunk, nchunks, nullptr, st));
+        } else {
+            S.kernel_launches += 1;
+            GSJ_CUDA(c, launch_item_counts(cell_start, nullptr, M, qchunk, nchunks, nullptr, st));
+        }
+        GSJ_TRY(dev_get(c, c->temp, scan_u32_u64_temp_bytes(M), (unsigned char**)&temp));
+        S.kernel_launches += 3;
+        GSJ_CUDA(c, scan_u32_u32(nchunks, item_off, M, temp, st));
+        GSJ_TRY(d2h_small(c, &num_items, item_off + M, 1));
+        S.work_items = num_items;
+        GSJ_TRY(dev_get(c, c->items, num_items, &items));
+        S.kernel_launches += 1;
+        GSJ_CUDA(c, launch_make_items(order, nchunks, item_off, M, items, st));
+    }
     GSJ_CUDA(c, cudaEventRecord(c->tev[1], st));
     GSJ_CUDA(c, cudaStreamSynchronize(st));
     const double t_join = now_ms();

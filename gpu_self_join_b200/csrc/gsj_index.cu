@@ -68,15 +68,35 @@ __global__ void k_minmax_partial(const T* __restrict__ in, uint64_t N, uint32_t 
     __shared__ T smin[kMaxK][32], smax[kMaxK][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     T mn[kMaxK], mx[kMaxK];
+    uint32_t col[kMaxK];
 #pragma unroll
     for (int j = 0; j < kMaxK; j++)
-        if (j < (int)k) mn[j] = mx[j] = in[perm[j]];
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
-         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (j < (int)k) {
+            col[j] = perm[j];
+            mn[j] = mx[j] = in[col[j]];
+        }
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    // four points per round, their loads issued together
+    for (; i + 3u * stride < N; i += 4u * stride) {
 #pragma unroll
         for (int j = 0; j < kMaxK; j++)
             if (j < (int)k) {
-                const T v = in[i * n + perm[j]];
+                T v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) v[u] = in[(i + (uint64_t)u * stride) * n + col[j]];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (v[u] < mn[j]) mn[j] = v[u];
+                    if (v[u] > mx[j]) mx[j] = v[u];
+                }
+            }
+    }
+    for (; i < N; i += stride) {
+#pragma unroll
+        for (int j = 0; j < kMaxK; j++)
+            if (j < (int)k) {
+                const T v = in[i * n + col[j]];
                 if (v < mn[j]) mn[j] = v;
                 if (v > mx[j]) mx[j] = v;
             }
@@ -112,19 +132,29 @@ __global__ void k_minmax_partial(const T* __restrict__ in, uint64_t N, uint32_t 
     }
 }
 
+// Warp j reduces dim j's partials (every partial starts from point 0's value,
+// so the strict comparisons keep the sequential semantics in any order).
 template <typename T>
 __global__ void k_minmax_final(const T* __restrict__ part, uint32_t nparts, uint32_t k,
                                T* __restrict__ out) {
-    const uint32_t j = threadIdx.x;
+    const uint32_t j = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     if (j >= k) return;
     T a = part[j], b = part[k + j];
-    for (uint32_t p = 1; p < nparts; p++) {
+    for (uint32_t p = lane; p < nparts; p += 32u) {
         const T a2 = part[(size_t)p * 2 * k + j], b2 = part[(size_t)p * 2 * k + k + j];
         if (a2 < a) a = a2;
         if (b2 > b) b = b2;
     }
-    out[j] = a;
-    out[k + j] = b;
+    for (int o = 16; o > 0; o >>= 1) {
+        const T a2 = __shfl_down_sync(0xffffffffu, a, o);
+        const T b2 = __shfl_down_sync(0xffffffffu, b, o);
+        if (a2 < a) a = a2;
+        if (b2 > b) b = b2;
+    }
+    if (lane == 0) {
+        out[j] = a;
+        out[k + j] = b;
+    }
 }
 
 // ------------------------------------------------------------ cell keys
@@ -282,7 +312,7 @@ template <typename T>
 cudaError_t launch_minmax(const T* in, uint64_t N, uint32_t n, uint32_t k, const uint32_t* perm, T* part,
                           uint32_t nparts, T* out, cudaStream_t st) {
     k_minmax_partial<T><<<nparts, 256, 0, st>>>(in, N, n, k, perm, part);
-    k_minmax_final<T><<<1, 32, 0, st>>>(part, nparts, k, out);
+    k_minmax_final<T><<<1, 32u * k, 0, st>>>(part, nparts, k, out);
     return cudaGetLastError();
 }
 

@@ -6,6 +6,9 @@
 //
 // Three phases over tiles of kScanTile elements: tile sums, a single-block
 // scan of the tile sums, and the tile-local scans with the tile prefix added.
+// Thread t of a tile owns its elements [16 t, 16 t + 16): four 16-byte loads
+// when the arrays are 16-byte aligned, one block-wide scan of the 256 thread
+// sums, then 16 sequential outputs per thread.
 // out has n+1 entries; out[n] is the total.
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -23,6 +26,7 @@ namespace gsj {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr uint64_t kScanTile = (uint64_t)kScanThreads * kScanItems;
+constexpr int kTileSumThreads = 1024;  // the single block scanning the tile sums
 
 __device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long x, int lane) {
 #pragma unroll
@@ -33,89 +37,117 @@ __device__ __forceinline__ unsigned long long warp_incl_scan(unsigned long long 
     return x;
 }
 
-// Block-wide exclusive scan of one value per thread; returns the exclusive
-// prefix and writes the block total to *total.
+// Block-wide exclusive scan of one value per thread (THREADS threads);
+// returns the exclusive prefix and writes the block total to *total.
+template <int THREADS>
 __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long* total) {
-    __shared__ unsigned long long wsum[kScanThreads / 32];
+    __shared__ unsigned long long wsum[THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned long long inc = warp_incl_scan(v, lane);
     if (lane == 31) wsum[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-        unsigned long long w = lane < kScanThreads / 32 ? wsum[lane] : 0ull;
+        unsigned long long w = lane < THREADS / 32 ? wsum[lane] : 0ull;
         w = warp_incl_scan(w, lane);
-        if (lane < kScanThreads / 32) wsum[lane] = w;
+        if (lane < THREADS / 32) wsum[lane] = w;
     }
     __syncthreads();
     const unsigned long long before = warp ? wsum[warp - 1] : 0ull;
-    *total = wsum[kScanThreads / 32 - 1];
+    *total = wsum[THREADS / 32 - 1];
     __syncthreads();
     return before + inc - v;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_tile_sums(const uint32_t* __restrict__ in, uint64_t n,
+// Elements [e0, e0 + kScanItems) (zero past n); vec: in is 16-byte aligned.
+__device__ __forceinline__ void load_items(const uint32_t* __restrict__ in, uint64_t e0, uint64_t n, bool vec,
+                                           uint32_t (&v)[kScanItems]) {
+    if (vec && e0 + kScanItems <= n) {
+        const uint4* p = reinterpret_cast<const uint4*>(in + e0);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; q++) {
+            const uint4 x = p[q];
+            v[4 * q] = x.x;
+            v[4 * q + 1] = x.y;
+            v[4 * q + 2] = x.z;
+            v[4 * q + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++) v[i] = e0 + (uint64_t)i < n ? in[e0 + i] : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_tile_sums(const uint32_t* __restrict__ in, uint64_t n, bool vec,
                                                             unsigned long long* __restrict__ tsum) {
-    const uint64_t base = blockIdx.x * kScanTile;
+    const uint64_t e0 = blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    load_items(in, e0, n, vec, v);
     unsigned long long s = 0;
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) {
-        const uint64_t e = base + (uint64_t)i * kScanThreads + threadIdx.x;
-        if (e < n) s += in[e];
-    }
+    for (int i = 0; i < kScanItems; i++) s += v[i];
     unsigned long long tot;
-    block_excl_scan(s, &tot);
+    block_excl_scan<kScanThreads>(s, &tot);
     if (threadIdx.x == 0) tsum[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(unsigned long long* __restrict__ tsum,
-                                                                 uint64_t ntiles) {
+// One block: tsum[i] becomes the exclusive prefix of the tile sums, tsum[ntiles]
+// the total.  Each thread takes 4 consecutive sums per round of 4096.
+__global__ void __launch_bounds__(kTileSumThreads) k_scan_tile_sums(unsigned long long* __restrict__ tsum,
+                                                                    uint64_t ntiles) {
     unsigned long long carry = 0;
-    for (uint64_t b0 = 0; b0 < ntiles; b0 += kScanThreads) {
-        const uint64_t i = b0 + threadIdx.x;
-        const unsigned long long v = i < ntiles ? tsum[i] : 0ull;
+    for (uint64_t b0 = 0; b0 < ntiles; b0 += 4u * kTileSumThreads) {
+        const uint64_t i0 = b0 + 4u * threadIdx.x;
+        unsigned long long v[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) v[j] = i0 + j < ntiles ? tsum[i0 + j] : 0ull;
         unsigned long long tot;
-        const unsigned long long ex = block_excl_scan(v, &tot);
-        if (i < ntiles) tsum[i] = carry + ex;
+        unsigned long long ex = block_excl_scan<kTileSumThreads>(v[0] + v[1] + v[2] + v[3], &tot);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (i0 + j < ntiles) tsum[i0 + j] = carry + ex;
+            ex += v[j];
+        }
         carry += tot;
     }
     if (threadIdx.x == 0) tsum[ntiles] = carry;
 }
 
 // OutT is uint64_t (list offsets) or uint32_t (slot offsets, digit offsets:
-// the caller guarantees that the total fits).  Warp w of the block owns the
-// tile's elements [w * 512, (w + 1) * 512), read and written as 16 rows of 32
-// consecutive elements (coalesced); each row is scanned across the lanes and
-// carried into the next.
+// the caller guarantees that the total fits).  vin / vout: in / out are
+// 16-byte aligned (a thread's 16 elements are then 4 aligned vectors in and
+// 4 or 8 out).
 template <typename OutT>
-__global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint32_t* __restrict__ in, uint64_t n,
+__global__ void __launch_bounds__(kScanThreads) k_tile_scan(const uint32_t* __restrict__ in, uint64_t n, bool vin,
                                                             const unsigned long long* __restrict__ tsum,
-                                                            uint64_t ntiles, OutT* __restrict__ out) {
-    __shared__ unsigned long long wtot[kScanThreads / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr uint64_t kWarpElems = kScanTile / (kScanThreads / 32);
-    const uint64_t base = blockIdx.x * kScanTile + (uint64_t)warp * kWarpElems + lane;
+                                                            uint64_t ntiles, OutT* __restrict__ out, bool vout) {
+    const uint64_t e0 = blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
+    load_items(in, e0, n, vin, v);
+    unsigned long long s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; i++) s += v[i];
+    unsigned long long tot;
+    unsigned long long pre = tsum[blockIdx.x] + block_excl_scan<kScanThreads>(s, &tot);
+    OutT o[kScanItems];
 #pragma unroll
     for (int i = 0; i < kScanItems; i++) {
-        const uint64_t e = base + (uint64_t)i * 32u;
-        v[i] = e < n ? in[e] : 0u;
+        o[i] = (OutT)pre;
+        pre += v[i];
     }
-    unsigned long long ex[kScanItems];
-    unsigned long long carry = 0;
+    if (vout && e0 + kScanItems <= n) {
+        if constexpr (sizeof(OutT) == 8) {
+            ulonglong2* p = reinterpret_cast<ulonglong2*>(out + e0);
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) {
-        const unsigned long long inc = warp_incl_scan(v[i], lane);
-        ex[i] = carry + inc - v[i];
-        carry += __shfl_sync(0xffffffffu, inc, 31);
-    }
-    if (lane == 0) wtot[warp] = carry;
-    __syncthreads();
-    unsigned long long pre = tsum[blockIdx.x];
-    for (int w = 0; w < warp; w++) pre += wtot[w];
+            for (int q = 0; q < kScanItems / 2; q++) p[q] = make_ulonglong2(o[2 * q], o[2 * q + 1]);
+        } else {
+            uint4* p = reinterpret_cast<uint4*>(out + e0);
 #pragma unroll
-    for (int i = 0; i < kScanItems; i++) {
-        const uint64_t e = base + (uint64_t)i * 32u;
-        if (e < n) out[e] = (OutT)(pre + ex[i]);
+            for (int q = 0; q < kScanItems / 4; q++) p[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kScanItems; i++)
+            if (e0 + (uint64_t)i < n) out[e0 + i] = o[i];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = (OutT)tsum[ntiles];
 }
@@ -127,9 +159,11 @@ static cudaError_t scan_any(const uint32_t* in, OutT* out, uint64_t n, void* tem
     const uint64_t ntiles = (n + kScanTile - 1) / kScanTile;
     unsigned long long* tsum = static_cast<unsigned long long*>(temp);
     if (ntiles == 0) return cudaMemsetAsync(out, 0, sizeof(OutT), st);
-    k_tile_sums<<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, tsum);
-    k_scan_tile_sums<<<1, kScanThreads, 0, st>>>(tsum, ntiles);
-    k_tile_scan<OutT><<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, tsum, ntiles, out);
+    const bool vin = (reinterpret_cast<uintptr_t>(in) & 15u) == 0;
+    const bool vout = (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
+    k_tile_sums<<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, vin, tsum);
+    k_scan_tile_sums<<<1, kTileSumThreads, 0, st>>>(tsum, ntiles);
+    k_tile_scan<OutT><<<(unsigned)ntiles, kScanThreads, 0, st>>>(in, n, vin, tsum, ntiles, out, vout);
     return cudaGetLastError();
 }
 

@@ -74,6 +74,33 @@ def test_noalloc_offsets_match_join_twice():
             assert int(got[-1]) == int(host_counts.sum(dtype=np.uint64)) == sj.total_pairs()
 
 
+@pytest.mark.parametrize("shift_in,shift_out", [(0, 0), (1, 0), (0, 1), (3, 1)])
+def test_noalloc_offsets_any_alignment_many_tiles(shift_in, shift_out):
+    """Counts and offsets at every 16-byte misalignment the element types allow
+    (the scan loads and stores whole 16-byte vectors only from aligned arrays),
+    over more than 4096 tiles of 4096 counts (the single-block scan of the tile
+    sums then takes two rounds) and a ragged last tile."""
+    import torch
+
+    from gpu_self_join_b200._native import lib
+
+    L = lib()
+    n = 4097 * 4096 + 1234
+    rng = np.random.default_rng(11 + shift_in + 2 * shift_out)
+    host = rng.integers(0, 3000, size=n, dtype=np.uint32)
+    cbuf = torch.from_numpy(np.concatenate([np.zeros(shift_in, np.uint32), host]).view(np.int32)).cuda()
+    obuf = torch.full((n + 1 + shift_out,), -1, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    rc = L.gsj_list_offsets_noalloc(ctypes.c_void_p(cbuf.data_ptr() + 4 * shift_in), n,
+                                    ctypes.c_void_p(obuf.data_ptr() + 8 * shift_out), None)
+    assert rc == 0, L.gsj_last_error(None)
+    torch.cuda.synchronize()
+    got = obuf.cpu().numpy().view(np.uint64)
+    want = np.concatenate([[0], np.cumsum(host, dtype=np.uint64)]).astype(np.uint64)
+    assert np.array_equal(got[shift_out:], want)
+    assert (got[:shift_out] == np.uint64(2**64 - 1)).all()  # nothing written before the output
+
+
 def test_noalloc_empty_input_writes_zero_total():
     """n = 0: the single offset (the total) is zero, whatever the output held."""
     import torch
