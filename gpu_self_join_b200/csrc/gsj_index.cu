@@ -9,6 +9,7 @@
 //   computeWorkDifficulty     GPU.cu:1491-1525   (k_item_* work items, heavy cells first)
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <type_traits>
 
 #include "gsj_common.cuh"
 #include "gsj_fp.cuh"
@@ -206,6 +207,31 @@ __global__ void k_gather_points(const T* __restrict__ in, uint64_t N, uint32_t n
     pts[e] = j < n ? in[(uint64_t)ids[s] * n + perm[j]] : T(0);
 }
 
+// The same for rows of npad = NP <= 4 entries: a thread per point, one id
+// load and the row stored as one vector.
+template <typename T, int NP>
+__global__ void k_gather_rows(const T* __restrict__ in, uint64_t N, uint32_t n, const uint32_t* __restrict__ perm,
+                              const uint32_t* __restrict__ ids, T* __restrict__ pts) {
+    const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    const T* src = in + (uint64_t)ids[s] * n;
+    T v[NP];
+#pragma unroll
+    for (int j = 0; j < NP; j++) v[j] = (uint32_t)j < n ? src[perm[j]] : T(0);
+    T* dst = pts + s * NP;
+    if constexpr (std::is_same<T, float>::value && NP == 2) {
+        *reinterpret_cast<float2*>(dst) = make_float2(v[0], v[1]);
+    } else if constexpr (std::is_same<T, float>::value && NP == 4) {
+        *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (std::is_same<T, double>::value && NP >= 2) {
+#pragma unroll
+        for (int j = 0; j < NP; j += 2) *reinterpret_cast<double2*>(dst + j) = make_double2(v[j], v[j + 1]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < NP; j++) dst[j] = v[j];
+    }
+}
+
 // ------------------------------------------------------------ cell lookup
 // Points per linear cell id (zero elsewhere); its exclusive scan is the
 // slot-prefix table ds: cell L holds slots [ds[L], ds[L+1]).
@@ -326,7 +352,10 @@ cudaError_t launch_cell_keys(const T* in, uint64_t N, uint32_t n, const uint32_t
 template <typename T>
 cudaError_t launch_gather_points(const T* in, uint64_t N, uint32_t n, uint32_t npad, const uint32_t* perm,
                                  const uint32_t* ids, T* pts, cudaStream_t st) {
-    k_gather_points<T><<<blocks_for(N * npad, 256), 256, 0, st>>>(in, N, n, npad, perm, ids, pts);
+    if (npad == 1) k_gather_rows<T, 1><<<blocks_for(N, 256), 256, 0, st>>>(in, N, n, perm, ids, pts);
+    else if (npad == 2) k_gather_rows<T, 2><<<blocks_for(N, 256), 256, 0, st>>>(in, N, n, perm, ids, pts);
+    else if (npad == 4) k_gather_rows<T, 4><<<blocks_for(N, 256), 256, 0, st>>>(in, N, n, perm, ids, pts);
+    else k_gather_points<T><<<blocks_for(N * npad, 256), 256, 0, st>>>(in, N, n, npad, perm, ids, pts);
     return cudaGetLastError();
 }
 

@@ -264,17 +264,23 @@ template cudaError_t radix_sort<uint32_t>(uint32_t*, uint32_t*, uint32_t*, uint3
 template cudaError_t radix_sort<uint64_t>(uint64_t*, uint64_t*, uint32_t*, uint32_t*, uint64_t, int, int, void*,
                                           bool*, int*, cudaStream_t);
 
-size_t runs_temp_bytes(uint64_t n) {
-    return (2 * (n + 1) * sizeof(uint32_t) + 255) / 256 * 256 + scan_u32_u64_temp_bytes(n) + 256;
+// flags[n + 1], then pos[n + 1] from the next 16-byte boundary (the scan moves
+// whole 16-byte vectors only between aligned arrays), then the scan's scratch.
+static uint64_t runs_pos_offset(uint64_t n) { return (n + 1 + 3) & ~3ull; }
+
+static size_t runs_arrays_bytes(uint64_t n) {
+    return ((runs_pos_offset(n) + n + 1) * sizeof(uint32_t) + 255) / 256 * 256;
 }
+
+size_t runs_temp_bytes(uint64_t n) { return runs_arrays_bytes(n) + scan_u32_u64_temp_bytes(n) + 256; }
 
 template <typename K>
 cudaError_t run_length(const K* keys, uint64_t n, uint64_t* run_key, uint32_t* run_start, uint32_t* d_nruns,
                        void* temp, cudaStream_t st) {
     if (n == 0) return cudaMemsetAsync(d_nruns, 0, sizeof(uint32_t), st);
     uint32_t* flags = static_cast<uint32_t*>(temp);
-    uint32_t* pos = flags + (n + 1);
-    void* stemp = static_cast<unsigned char*>(temp) + (2 * (n + 1) * sizeof(uint32_t) + 255) / 256 * 256;
+    uint32_t* pos = flags + runs_pos_offset(n);
+    void* stemp = static_cast<unsigned char*>(temp) + runs_arrays_bytes(n);
     k_run_flags<K><<<blocks_for(n, 256), 256, 0, st>>>(keys, n, flags);
     cudaError_t e = scan_u32_u32(flags, pos, n, stemp, st);
     if (e != cudaSuccess) return e;
