@@ -39,7 +39,7 @@
 // alternate, handed over by mbarriers only (staged: every producer thread's
 // slots and landed rows of a buffer; full: MMA commit + the issuer's release;
 // empty and free: the consumer arrivals), so the producer warps never wait for
-// one another.  Every wait is a bounded poll by one thread whose verdict is
+// one another.  Every wait is a bounded poll by one thread whose outcome is
 // shared before any warp-collective; on time-out the error flag is raised and
 // the CTA stops.  Tensor memory (2 x 128 columns) is allocated once
 // per CTA; the shared-memory request keeps at most 2 CTAs (512 columns) on an
