@@ -62,3 +62,15 @@ def test_screen_path_is_a_tensor_roofline():
 
 def test_traffic_lookup_missing_profile():
     assert bench._traffic_from_profile("no_such_kernel", "c2_gmm2d") is None
+
+
+def test_traffic_of_the_committed_fill_profile():
+    """The fill capture's DRAM traffic, scaled to the 20M-point launch, lies between the
+    algorithmic bytes of that launch and a few times them (a figure left unscaled from the
+    8M-point capture, or one of another kernel, would fall outside)."""
+    w = synth.WORKLOADS["c2_gmm2d"]
+    R, C = 642_337_374, 1_802_646_654
+    traffic = bench._traffic_from_profile("join_fill", "c2_gmm2d")
+    assert traffic is not None
+    alg = 4.0 * R + 24.0 * w.N + C / 8.0
+    assert alg < traffic < 6.0 * alg
